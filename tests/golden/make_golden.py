@@ -1,0 +1,212 @@
+"""Generates the golden fixtures in this directory by running the reference itself.
+
+The reference (dhidas/SRSOriginal, OSCARS SR 1.31.05) is built from its own sources by
+``make -C oracle reference`` into ``oracle/_ref/`` (module ``sr``); this script imports it, runs the
+hot-path calls on seeded synthetic inputs and stores the outputs as compressed ``.npz`` files.  It
+needs the reference sources, so it runs only where they are mounted; the fixtures it writes are
+committed and are all the tests need.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import io
+import json
+import math
+import os
+import sys
+import tempfile
+from contextlib import redirect_stdout
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+
+from srsoriginal_b200 import workloads as W  # noqa: E402
+
+NT = os.cpu_count() or 2
+
+
+def new_sr():
+    with redirect_stdout(io.StringIO()):
+        import sr  # the reference, built by oracle/Makefile
+    return sr.sr()
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **{k: np.asarray(v) for k, v in arrays.items()})
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def traj_arrays(tr):
+    t = np.asarray(tr, dtype=np.float64)  # (n, 2, 3)
+    return t[:, 0, :].T.copy(), t[:, 1, :].T.copy()
+
+
+def values(lst):
+    return np.array([p[1] for p in lst], dtype=np.float64)
+
+
+def coords(lst):
+    return np.array([p[0] for p in lst], dtype=np.float64)
+
+
+def cfg0():
+    o = new_sr()
+    W.setup_beam(o, 20001)
+    W.setup_undulator(o)
+    X, B = traj_arrays(o.calculate_trajectory())
+    s = np.array(o.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], npoints=1000,
+                                      energy_range_eV=[100, 1000], nthreads=NT))
+    power = o.calculate_total_power()
+    # small companion case (full trajectory stored)
+    o2 = new_sr()
+    W.setup_beam(o2, 2001)
+    W.setup_undulator(o2)
+    Xs, Bs = traj_arrays(o2.calculate_trajectory())
+    ss = np.array(o2.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], npoints=64,
+                                        energy_range_eV=[100, 1000], nthreads=1))
+    save("spectrum_cfg0.npz", energies=s[:, 0], flux=s[:, 1], x_sub=X[:, ::50], beta_sub=B[:, ::50],
+         x_last=X[:, -1], beta_last=B[:, -1], n=X.shape[1], total_power=power,
+         small_x=Xs, small_beta=Bs, small_energies=ss[:, 0], small_flux=ss[:, 1],
+         small_total_power=o2.calculate_total_power())
+    k = int(np.argmax(np.where(s[:, 0] < 300, s[:, 1], 0)))
+    return float(s[k, 0])
+
+
+def cfg1(e1):
+    out = {}
+    for tag, e in (("e1", e1), ("e3", 3 * e1)):
+        o = new_sr()
+        W.setup_beam(o, 20001)
+        W.setup_undulator(o)
+        m = o.calculate_flux_rectangle(plane="XY", energy_eV=e, width=[0.01, 0.01],
+                                       npoints=[101, 101], translation=[0, 0, W.SCREEN_Z], nthreads=NT)
+        out["flux_" + tag] = values(m)
+        out["x12"] = coords(m)[:, :2]
+        out["energy_" + tag] = e
+    save("flux_cfg1.npz", **out)
+
+
+def cfg2():
+    o = new_sr()
+    W.setup_beam(o, 40001)
+    W.setup_epu(o)
+    m = o.calculate_power_density_rectangle(plane="XY", width=[0.04, 0.04], npoints=[201, 201],
+                                            translation=[0, 0, W.SCREEN_Z], nthreads=NT)
+    n = 201 * 201
+    save("pd_cfg2.npz", pd=values(m)[:n], x12=coords(m)[:n, :2], total_power=o.calculate_total_power(),
+         nlist=len(m))
+
+
+def misc():
+    """Other field kinds, rotations, surfaces and the directional power density."""
+    o = new_sr()
+    W.setup_beam(o, 3001)
+    o.add_bfield_undulator(bfield=[0, 0.8, 0.05], period=[0, 0, 0.05], nperiods=11, phase=0.3,
+                           rotations=[0.001, -0.002, 0.3], translation=[0.0001, 0, 0.05], taper=0.01)
+    o.add_bfield_gaussian(bfield=[0.02, 0.3, 0], sigma=[0, 0, 0.05], translation=[0, 0, -0.5],
+                          rotations=[0, 0.01, 0])
+    o.add_bfield_uniform(bfield=[0.0, -0.01, 0.001], width=[0, 0, 0.2], translation=[0, 0, 0.5],
+                         rotations=[0.02, 0, 0])
+    X, B = traj_arrays(o.calculate_trajectory())
+    s = np.array(o.calculate_spectrum(obs=[0.001, -0.0005, 20], npoints=40,
+                                      energy_range_eV=[50, 2000], nthreads=1))
+    sp = np.array(o.calculate_spectrum(obs=[0.0, 0.0, 25], points_eV=[75.0, 133.3, 401.0, 999.9],
+                                       nthreads=1))
+    bf = np.array([o.get_bfield([0.0001 * i, -0.0002 * i, -1 + 0.1 * i]) for i in range(21)])
+    pd1 = o.calculate_power_density_rectangle(plane="YZ", width=[0.02, 0.03], npoints=[7, 9],
+                                              rotations=[0, -math.pi / 2, 0],
+                                              translation=[0.001, 0, 20], normal=1, nthreads=1)
+    pdm = o.calculate_power_density_rectangle(plane="YZ", width=[0.02, 0.03], npoints=[7, 9],
+                                              rotations=[0, -math.pi / 2, 0],
+                                              translation=[0.001, 0, 20], normal=-1, nthreads=1)
+    fx = o.calculate_flux_rectangle(energy_eV=300.0, npoints=[6, 5],
+                                    x0x1x2=[[-0.004, -0.003, 25], [0.004, -0.003, 25], [-0.004, 0.003, 25.1]],
+                                    nthreads=1, dim=3)
+    save("misc_fields.npz", x=X, beta=B, energies=s[:, 0], flux=s[:, 1], pts_energies=sp[:, 0],
+         pts_flux=sp[:, 1], bfield=bf, pd_dir=values(pd1), pd_dir_xyz=coords(pd1), pd_neg=values(pdm),
+         flux_x0x1x2=values(fx)[:30], flux_x0x1x2_xyz=coords(fx)[:30], flux_x0x1x2_len=len(fx),
+         total_power=o.calculate_total_power())
+
+
+def beam():
+    """Twiss-sampled particles (config 3a beam) from set_seed(0), and a 4-particle spectrum."""
+    o = new_sr()
+    W.setup_beam(o, 2001, **W.BEAM_3A)
+    W.setup_undulator(o)
+    o.set_seed(0)
+    x0, b0 = [], []
+    for _ in range(33):
+        o.set_new_particle(particle="random")
+        x0.append(o.get_particle_x0())
+        b0.append(o.get_particle_beta0())
+    o.set_seed(0)
+    s = np.array(o.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], npoints=48, energy_range_eV=[100, 1000],
+                                      nparticles=4, nthreads=1))
+    o.set_seed(0)
+    f = o.calculate_flux_rectangle(plane="XY", energy_eV=W.E1_EV, width=[0.01, 0.01], npoints=[5, 5],
+                                   translation=[0, 0, W.SCREEN_Z], nparticles=3, nthreads=1)
+    o.set_seed(0)
+    p = o.calculate_power_density_rectangle(plane="XY", width=[0.04, 0.04], npoints=[5, 5],
+                                            translation=[0, 0, W.SCREEN_Z], nparticles=3, nthreads=1)
+    o.set_seed(7.9)
+    u = [o.rand() for _ in range(5)] + [o.norm() for _ in range(5)]
+    save("beam_3a.npz", x0=np.array(x0), beta0=np.array(b0), energies=s[:, 0], flux=s[:, 1],
+         flux_map=values(f), flux_map_len=len(f), pd_map=values(p), pd_map_len=len(p), draws=np.array(u))
+
+
+def grid():
+    """Config 4 field from an OSCARS-format grid file."""
+    z, by = W.config4_grid()
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "cfg4.txt")
+        W.write_oscars_grid(path, z, by)
+        o = new_sr()
+        W.setup_beam(o, 20001)
+        o.add_bfield_file(ifile=path, iformat="OSCARS")
+        X, B = traj_arrays(o.calculate_trajectory())
+        e3 = W.E3_EV
+        s = np.array(o.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], npoints=200,
+                                          energy_range_eV=[0.98 * e3, 1.02 * e3], nthreads=NT))
+        bf = np.array([o.get_bfield([0, 0, -0.9 + 0.0123 * i]) for i in range(150)])
+    save("grid_cfg4.npz", by=by, x_sub=X[:, ::50], beta_sub=B[:, ::50], x_last=X[:, -1], n=X.shape[1],
+         energies=s[:, 0], flux=s[:, 1], bfield=bf)
+
+
+def quirks():
+    """Output-list lengths of the dispatch paths (reference behaviour, kept by the drop-in)."""
+    res = {}
+    for nthreads in (1, 2):
+        o = new_sr()
+        W.setup_beam(o, 501)
+        W.setup_undulator(o)
+        f = o.calculate_flux_rectangle(plane="XY", energy_eV=150.0, width=[0.01, 0.01], npoints=[3, 4],
+                                       translation=[0, 0, 30], nthreads=nthreads)
+        p = o.calculate_power_density_rectangle(plane="XY", width=[0.01, 0.01], npoints=[3, 4],
+                                                translation=[0, 0, 30], nthreads=nthreads)
+        p3 = o.calculate_power_density_rectangle(plane="XY", width=[0.01, 0.01], npoints=[3, 4],
+                                                 translation=[0, 0, 30], nthreads=nthreads, dim=3)
+        res[f"flux_len_nthreads{nthreads}"] = len(f)
+        res[f"pd_len_nthreads{nthreads}"] = len(p)
+        res[f"pd_dim3_first_nthreads{nthreads}"] = p3[0][0]
+        res[f"flux_coords_nthreads{nthreads}"] = [q[0] for q in f]
+    with open(os.path.join(HERE, "quirks.json"), "w") as fh:
+        json.dump(res, fh, indent=1)
+
+
+if __name__ == "__main__":
+    e1 = cfg0()
+    print("E1 (first-harmonic peak of the config-0 spectrum):", repr(e1))
+    if abs(e1 - W.E1_EV) > 1e-9:
+        print("NOTE: update workloads.E1_EV to", repr(e1))
+    cfg1(e1)
+    cfg2()
+    misc()
+    beam()
+    grid()
+    quirks()
