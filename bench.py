@@ -1,0 +1,365 @@
+"""Benchmark: flux maps of the config-1 workload on the B200.
+
+Workload (config 1): 3 GeV, 0.5 A electron, ideal planar undulator (1 T, 49 mm, 31 periods), RK4
+trajectory of 20001 points over ct in [0, 2] m from z = -1 m; flux on a 10 mm x 10 mm XY rectangle at
+z = 30 m, 101 x 101 points, at the first harmonic (E1 = 152.25 eV, the peak of the config-0
+spectrum) and at 3*E1.  Synthetic inputs (no dataset).
+
+One step = both flux maps (E1 and E3) in mixed precision from the device-resident trajectory:
+2 * 20001 * 10201 = 4.08e8 integrand evaluations.  ``value`` is integrand evaluations per second of
+the whole job (all ranks), device-timed with CUDA events per step; the L2 (126 MB) is flushed with a
+256 MiB write before every step, outside the timed events.  ``e2e`` is the same metric through the
+public API (``srsoriginal_b200.sr.sr``: RK4 trajectory on the GPU, host->device copies of the inputs,
+both maps, device->host copy of the results), host wall-clock around synchronous calls.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NT = 20001
+GRID_N = 101
+WIDTH = 0.01
+E1 = 152.25225225225225
+ENERGIES = (E1, 3 * E1)
+EVALS_PER_STEP = len(ENERGIES) * NT * GRID_N * GRID_N
+METRIC = "integrand evals/s (mixed vs plain FP64 at <=1e-4 rel flux err)"
+UNIT = "evals/s"
+
+# Algorithmic work per integrand evaluation of the mixed flux kernel (per (trajectory point,
+# observation point) pair; FP32 instructions with an FMA counted as one, MUFU ops, FP64 instructions).
+# Per pair: D_j - D_c (g: 3, h: 1, second-order term: 3, total: 1), 1/D_j (1 + 1 MUFU), phase (3),
+# reduction mod 2pi (5), sincos (1 + 2 MUFU), n_j - n_c (6), amplitude (9), complex MAC (12).
+# The per-(trajectory point, tile) FP64 anchor (~60 FP64 instructions per 128 pairs) is < 0.5 per pair.
+OPS_PER_EVAL = {"fp32": 45.0, "sfu": 3.0, "fp64": 0.5}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ distributed plumbing
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------ CPU baseline (the reference)
+
+def reference_module():
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+    import io
+    from contextlib import redirect_stdout
+    with redirect_stdout(io.StringIO()):
+        import sr as ref_sr  # the reference built from its own sources by oracle/Makefile
+    return ref_sr
+
+
+def reference_sample(rows, threads):
+    """The reference's CPU path (nthreads = host threads) on a sample of the workload: the full
+    trajectory and both energies, on `rows` rows of the 101 x 101 map.  Returns (seconds, evals)."""
+    from srsoriginal_b200 import workloads as W
+    ref_sr = reference_module()
+    o = ref_sr.sr()
+    W.setup_beam(o, NT)
+    W.setup_undulator(o)
+    h = WIDTH * (rows - 1) / (GRID_N - 1)
+    t0 = time.perf_counter()
+    for e in ENERGIES:
+        o.calculate_flux_rectangle(plane="XY", energy_eV=e, width=[WIDTH, h if rows > 1 else WIDTH],
+                                   npoints=[GRID_N, rows], translation=[0, 0, W.SCREEN_Z], nthreads=threads)
+    return time.perf_counter() - t0, len(ENERGIES) * NT * GRID_N * rows
+
+
+def cpu_baseline(target_s=10.0):
+    threads = os.cpu_count() or 1
+    dt, ev = reference_sample(2, threads)  # calibration
+    rows = max(2, min(GRID_N, int(2 * target_s / max(dt, 1e-3))))
+    dt, ev = reference_sample(rows, threads)
+    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"reference CPU path (oracle/_ref, nthreads={threads}): full 20001-point trajectory, "
+                      f"both energies, {GRID_N} x {rows} of the 101 x 101 map ({ev:.3g} evals, {dt:.1f} s)"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    dt, ev = reference_sample(2, threads)
+    # each step: a bounded sample sized so warmup + steps stay within a few minutes
+    per_step_target = max(1.0, 150.0 / max(1, args.steps + args.warmup))
+    rows = max(2, min(GRID_N, int(2 * per_step_target / max(dt, 1e-3))))
+    for _ in range(args.warmup):
+        reference_sample(rows, threads)
+    times, evals = [], 0
+    for _ in range(args.steps):
+        dt, ev = reference_sample(rows, threads)
+        times.append(dt)
+        evals = ev
+    tot = sum(times)
+    value = evals * args.steps / tot
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "config 1: flux maps 101x101 at E1 and 3*E1, 20001-point trajectory "
+                                   f"(each step a {GRID_N} x {rows} sample of each map)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{GRID_N} x {rows} rows of each map, both energies, full trajectory"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from srsoriginal_b200 import _lib, device as D, workloads as W
+    from srsoriginal_b200.sr import rectangle_points, sr
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    fields = [D.undulator([0, W.BPEAK, 0], [0, 0, W.PERIOD], W.NPERIODS)]
+    part, gamma = D.ideal_particle(W.ENERGY_GEV, [0, 0, -1], [0, 0, 1])
+    traj = D.trajectory(fields, [part], 0.0, 2.0, 0.0, NT)
+    xyz, x12, nrm, grid = rectangle_points([GRID_N, GRID_N], "XY", [WIDTH, WIDTH], translation=[0, 0, W.SCREEN_Z])
+    pts = torch.as_tensor(np.ascontiguousarray(xyz.reshape(-1)), device=dev)
+    npts = GRID_N * GRID_N
+    out = {e: torch.empty(npts, dtype=torch.float64, device=dev) for e in ENERGIES}
+    out64 = {e: torch.empty(npts, dtype=torch.float64, device=dev) for e in ENERGIES}
+    charge, current = -D.QE, W.CURRENT
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    # trajectory time (one RK4 launch, single particle), for the record
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    D.trajectory(fields, [part], 0.0, 2.0, 0.0, NT, out=traj)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    rk4_ms = e0.elapsed_time(e1)
+
+    def step(precision, outs):
+        for e in ENERGIES:
+            D.flux(traj, charge, current, e, outs[e], points=pts, grid=grid, precision=precision)
+
+    def timed(precision, outs, steps, warmup):
+        for _ in range(warmup):
+            step(precision, outs)
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        evs = []
+        for _ in range(steps):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(precision, outs)
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs)
+
+    # plain FP64 kernel on the same workload: the denominator of the mixed/plain ratio and the check
+    # of the mixed maps' error
+    fp64_ms = timed(_lib.FP64, out64, max(1, min(3, args.steps)), 1) / max(1, min(3, args.steps))
+    clocks = ClockSampler(local)
+    clocks.start()
+    total_ms = timed(_lib.MIXED, out, args.steps, args.warmup)
+    clk = clocks.stop()
+    total_ms = max_over_ranks(total_ms, world)
+    ms_per_step = total_ms / args.steps
+    value = world * EVALS_PER_STEP / (ms_per_step * 1e-3)
+
+    # accuracy of the mixed maps against the plain FP64 maps (the drop-in)
+    err = {}
+    for e in ENERGIES:
+        a, b = out[e].cpu().numpy(), out64[e].cpu().numpy()
+        big = np.abs(b) >= 1e-3 * np.abs(b).max()
+        err[f"{e:.2f}eV"] = {"max_rel_over_1e-3max": float(np.max(np.abs(a[big] - b[big]) / np.abs(b[big]))),
+                             "rms_rel_over_1e-3max": float(np.sqrt(np.mean(((a[big] - b[big]) / b[big]) ** 2))),
+                             "normwise": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
+
+    # roofline of the dominant kernel (mixed flux): algorithmic ops per launch / launch time
+    import ctypes
+    peaks = {}
+    for kind, name in ((0, "fp32"), (1, "fp64"), (2, "sfu")):
+        v = ctypes.c_double()
+        _lib.check(_lib.lib.srs_measure_peak(kind, ctypes.byref(v), ctypes.c_void_p(stream.cuda_stream)))
+        peaks[name] = v.value
+    evals_per_launch = NT * npts
+    launch_s = ms_per_step * 1e-3 / len(ENERGIES)
+    bounds = {k: OPS_PER_EVAL[k] * evals_per_launch / peaks[k] for k in peaks}
+    bound = max(bounds, key=bounds.get)
+    achieved = OPS_PER_EVAL[bound] * evals_per_launch / launch_s
+    roofline = {"bound": bound, "achieved": achieved / 1e12, "peak": peaks[bound] / 1e12, "unit": "Tops/s",
+                "frac": achieved / peaks[bound], "traffic": None,
+                "peak_source": "measured live (srs_measure_peak: FFMA / DFMA / MUFU chains, all SMs)",
+                "ops_per_eval": OPS_PER_EVAL, "evals_per_launch": evals_per_launch,
+                "all_peaks_Tops": {k: v / 1e12 for k, v in peaks.items()}}
+    traffic_file = os.path.join(ROOT, "profiles", "flux_mixed_cfg1_traffic.json")
+    if os.path.exists(traffic_file):
+        roofline["traffic"] = json.load(open(traffic_file)).get("bytes_per_launch")
+
+    # e2e through the public API (host buffers, synchronous calls)
+    o = sr()
+    W.setup_beam(o, NT)
+    W.setup_undulator(o)
+    e2e_steps = max(1, min(args.steps, 10))
+    for _ in range(min(2, args.warmup)):
+        for e in ENERGIES:
+            o.flux_arrays(e, [GRID_N, GRID_N], "XY", [WIDTH, WIDTH], translation=[0, 0, W.SCREEN_Z],
+                          precision="mixed")
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for e in ENERGIES:
+            o.flux_arrays(e, [GRID_N, GRID_N], "XY", [WIDTH, WIDTH], translation=[0, 0, W.SCREEN_Z],
+                          precision="mixed")
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = {"value": world * EVALS_PER_STEP * e2e_steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": len(ENERGIES) * (npts * 3 * 8 + 2 * npts * 8 + 248 + 56),
+           "d2h_bytes_per_step": len(ENERGIES) * 2 * npts * 8,
+           "ms_per_step": 1e3 * e2e_s / e2e_steps,
+           "includes": "RK4 trajectory on the GPU per map, H2D of points/fields/particle/accumulators, both "
+                       "maps, D2H of results"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic",
+            "config": {"workload": "config 1: flux maps 101x101 (10 mm square at 30 m) at E1=152.25 eV and "
+                                   "3*E1, 20001-point trajectory, 3 GeV 0.5 A, 1 T / 49 mm / 31-period undulator",
+                       "evals_per_step": EVALS_PER_STEP, "precision": "mixed",
+                       "l2": "256 MiB write before every step, outside the per-step CUDA events",
+                       "parallelism": f"replicas x{world} (weak)"},
+            "fp64_plain": {"value": EVALS_PER_STEP / (fp64_ms * 1e-3), "unit": UNIT, "ms_per_step": fp64_ms},
+            "mixed_over_fp64": (EVALS_PER_STEP / (ms_per_step * 1e-3)) / (EVALS_PER_STEP / (fp64_ms * 1e-3)),
+            "mixed_error_vs_fp64": err,
+            "rk4_trajectory_ms": rk4_ms,
+            "roofline": roofline, "clocks": clk, "e2e": e2e,
+            "gpu_launches": args.steps * len(ENERGIES) * 2}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline()
+        except Exception as ex:  # the reference module is built here only when its sources exist
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": f"unavailable: {ex}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":  # host-only: rank 0 runs the reference's CPU path, other ranks exit
+        return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+    world, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,297 @@
+/*
+ * srs_b200 -- B200-native radiation hot path of the SRS / OSCARS synchrotron-radiation simulator:
+ * the RK4 electron trajectory through magnetic fields and the frequency-domain Lienard-Wiechert sums
+ * (on-axis spectrum, flux on a surface, power density on a surface).
+ *
+ * Plain C ABI: POD structs, plain pointers and sizes, no C++ or torch types.  Every call returns an
+ * srs_status; srs_last_error() returns the message of the calling thread's last failure.  No
+ * exception crosses this boundary.
+ *
+ * Reference interfaces replaced (paths inside dhidas/SRSOriginal):
+ *   include/OSCARSSR_Cuda.h:25  OSCARSSR_Cuda_GetDeviceCount            -> srs_device_count
+ *   include/OSCARSSR_Cuda.h:27  OSCARSSR_Cuda_CalculateSpectrumGPU      -> srs_spectrum
+ *   include/OSCARSSR_Cuda.h:26  OSCARSSR_Cuda_CalculateFluxGPU          -> srs_flux
+ *   include/OSCARSSR_Cuda.h:28  OSCARSSR_Cuda_CalculatePowerDensityGPU  -> srs_power_density
+ *   src/OSCARSSR.cc:562-874     OSCARSSR::CalculateTrajectory + RK4     -> srs_trajectory
+ *   src/OSCARSSR.cc:1939-1978   OSCARSSR::CalculateTotalPower           -> srs_total_power
+ * and, for the Python-facing calls of src/OSCARSSR_Python.cc, the srs_sim_* object API below.
+ *
+ * Units follow the reference: SI, energies in eV (photons) and GeV (beam), times as c*t in metres,
+ * flux in photons/s/0.1%bw/mm^2, power density in W/mm^2.
+ */
+#ifndef SRS_B200_H
+#define SRS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int srs_status;
+enum {
+  SRS_OK = 0,
+  SRS_ERR_INVALID = 1,   /* bad argument (reference: ValueError / std::invalid_argument) */
+  SRS_ERR_RANGE = 2,     /* out of range / length (reference: std::out_of_range, length_error) */
+  SRS_ERR_CUDA = 3,      /* a CUDA runtime error; the message names the call */
+  SRS_ERR_NO_DEVICE = 4, /* no CUDA device */
+  SRS_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+  SRS_ERR_IO = 6         /* a field file could not be read */
+};
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char *srs_last_error(void);
+/* Library version string. */
+const char *srs_version(void);
+
+/* Number of CUDA devices (OSCARSSR_Cuda_GetDeviceCount, src/OSCARSSR_Cuda.cu:30-36). */
+int srs_device_count(void);
+
+/* ------------------------------------------------------------------ fields */
+
+enum { SRS_FIELD_UNDULATOR = 1, SRS_FIELD_GAUSSIAN = 2, SRS_FIELD_UNIFORM_BOX = 3, SRS_FIELD_GRID = 4 };
+
+/* One magnetic-field object in the form the reference keeps after construction:
+ *  undulator (TField3D_IdealUndulator.cc): field and period already rotated, center, nperiods,
+ *            phase [rad], taper [1/m];
+ *  gaussian  (TField3D_Gaussian.cc): field already rotated, center, sigma (axes with sigma<=0 are
+ *            ignored), rotations applied to the evaluation point;
+ *  uniform box (TField3D_UniformBox.cc): field rotated, center, width (<=0: unbounded axis),
+ *            rotations applied to the point;
+ *  grid (TField3D_Grid.cc): rotations and translation applied to the point, start/step/n per axis,
+ *            data = 3 doubles per sample at index ix*ny*nz + iy*nz + iz, already rotated.  For
+ *            srs_trajectory the data pointer must be DEVICE memory; the srs_sim_* API owns its copy. */
+typedef struct srs_field {
+  int32_t kind;
+  int32_t nperiods;
+  double field[3];
+  double period[3];
+  double center[3];
+  double phase;
+  double taper;
+  double sigma_or_width[3];
+  double rotations[3];
+  double translation[3];
+  double start[3];
+  double step[3];
+  int64_t n[3];
+  const double *data;
+} srs_field;
+
+/* Initial conditions of one particle: position [m], beta = v/c, q/(m gamma) [C/kg]. */
+typedef struct srs_particle {
+  double x0[3];
+  double beta0[3];
+  double qomg;
+} srs_particle;
+
+/* ------------------------------------------------------------------ trajectory */
+
+/* Time step and point counts of the reference's forward/backward RK4 (OSCARSSR.cc:592-598):
+ * dt = (ctstop-ctstart)/c/(npoints-1), nforward = (size_t)(1 + (ctstop-t0)/c/dt),
+ * nbackward = (size_t)((t0-ctstart)/c/dt); a trajectory has nforward+nbackward points. */
+srs_status srs_trajectory_counts(double ctstart, double ctstop, double t0, int64_t npoints, double *dt,
+                                 int64_t *nforward, int64_t *nbackward);
+
+/* Fixed-step RK4 of nparticles particles through the sum of the fields, one CUDA thread per
+ * particle, in the reference's IEEE-double operation order (OSCARSSR.cc:562-874).  particles and
+ * fields are HOST arrays; d_x, d_beta, d_aoc are DEVICE arrays of nparticles*3*n doubles laid out
+ * [particle][component][point] (n = nforward+nbackward).  The stored a/c of a point is the derivative
+ * at the previous step's state, as in the reference (0 at the first forward point).  stream: a
+ * cudaStream_t or NULL. */
+srs_status srs_trajectory(const srs_field *fields, int32_t nfields, const srs_particle *particles,
+                          int32_t nparticles, double ctstart, double ctstop, double t0, int64_t npoints,
+                          double *d_x, double *d_beta, double *d_aoc, void *stream);
+
+/* ------------------------------------------------------------------ radiation sums */
+
+/* Arithmetic of the sums. */
+enum {
+  SRS_PRECISION_FP64 = 0, /* plain IEEE double, the reference's operation order: the drop-in */
+  SRS_PRECISION_MIXED = 1 /* FP32 amplitude/sincos/accumulation, FP64 phase and reduction */
+};
+
+/* Trajectory of one or more particles on the DEVICE, layout as written by srs_trajectory. */
+typedef struct srs_traj_view {
+  const double *x;
+  const double *beta;
+  const double *aoc;
+  int64_t n;          /* points per particle */
+  int32_t nparticles; /* particles, consecutive blocks of 3*n doubles */
+  double dt;          /* time step [s] */
+} srs_traj_view;
+
+/* Beam constants of the sums: particle charge [C] and beam current [A]. */
+typedef struct srs_beam_consts {
+  double charge;
+  double current;
+} srs_beam_consts;
+
+/* Flux spectrum at one observer (OSCARSSR_Cuda_CalculateSpectrumGPU / OSCARSSR.cc:1154-1251):
+ * d_energies (DEVICE, ne photon energies in eV).  d_out (DEVICE) receives nparticles*ne values,
+ * particle-major: flux of each particle (weight 1).  Mixed precision walks uniform energy grids with
+ * a complex-rotation recurrence; non-uniform grids get one sincos per term. */
+srs_status srs_spectrum(srs_traj_view traj, srs_beam_consts beam, const double obs[3],
+                        const double *d_energies, int64_t ne, int32_t precision, double *d_out,
+                        void *stream);
+
+/* Flux at np observation points at one photon energy (OSCARSSR_Cuda_CalculateFluxGPU /
+ * OSCARSSR.cc:1989-2099).  d_points: DEVICE, 3*np doubles (x,y,z per point).  d_out: DEVICE,
+ * nparticles*np values.  For SRS_PRECISION_MIXED the points must form a regular grid given by grid
+ * (see srs_grid2d) and d_points may be NULL. */
+typedef struct srs_grid2d {
+  double origin[3]; /* point (0,0) */
+  double u1[3];     /* step to point (1,0) */
+  double u2[3];     /* step to point (0,1) */
+  double normal[3]; /* unit surface normal (power density) */
+  int32_t n1, n2;   /* point i is (i / n2, i % n2), as TSurfacePoints_Rectangle::GetXYZ */
+} srs_grid2d;
+
+srs_status srs_flux(srs_traj_view traj, srs_beam_consts beam, const double *d_points, int64_t np,
+                    const srs_grid2d *grid, double energy_ev, int32_t precision, double *d_out,
+                    void *stream);
+
+/* Power density at np points with unit normals (OSCARSSR.cc:1477-1598; the reference's CPU
+ * semantics: with directional != 0 the terms with n.normal <= 0 are skipped, otherwise the result is
+ * made non-negative).  d_points, d_normals: DEVICE 3*np doubles.  d_out: DEVICE nparticles*np values
+ * in W/mm^2 (weight 1).  For SRS_PRECISION_MIXED the points must form the regular grid `grid`
+ * (normal included) and d_points/d_normals may be NULL. */
+srs_status srs_power_density(srs_traj_view traj, srs_beam_consts beam, const double *d_points,
+                             const double *d_normals, int64_t np, const srs_grid2d *grid,
+                             int32_t directional, int32_t precision, double *d_out, void *stream);
+
+/* Total radiated power of each particle (OSCARSSR.cc:1939-1978); gamma is per particle (HOST array).
+ * out: HOST, nparticles values [W]. */
+srs_status srs_total_power(srs_traj_view traj, srs_beam_consts beam, const double *gamma, double *out,
+                           void *stream);
+
+/* Deterministic weighted sum over particles: out[j] (HOST) += w * Kahan-accumulated values
+ * d_vals[p*nout + j] in particle order, with the reference containers' compensation array comp
+ * (HOST, nout), i.e. exactly the reference's per-particle AddToFlux/AddToPoint sequence. */
+srs_status srs_accumulate(const double *d_vals, int32_t nparticles, int64_t nout, double weight,
+                          double *out, double *comp, void *stream);
+
+/* ------------------------------------------------------------------ simulation object
+ * The state and calls behind the reference's Python type oscars.sr.sr (src/OSCARSSR_Python.cc),
+ * for the hot-path methods.  One object per thread; calls on one object are serialised. */
+typedef struct srs_sim srs_sim;
+
+srs_status srs_sim_create(srs_sim **out);
+void srs_sim_destroy(srs_sim *sim);
+
+srs_status srs_sim_set_ctstartstop(srs_sim *sim, double start, double stop);       /* :282 */
+srs_status srs_sim_set_npoints_trajectory(srs_sim *sim, int64_t n);                 /* :315 */
+srs_status srs_sim_get_ctstartstop(srs_sim *sim, double *start, double *stop);
+int64_t srs_sim_get_npoints_trajectory(srs_sim *sim);
+srs_status srs_sim_set_nthreads_global(srs_sim *sim, int32_t n);                    /* :239 */
+srs_status srs_sim_set_gpu_global(srs_sim *sim, int32_t g);                         /* :200 */
+
+/* Fields (:736 undulator, :561 gaussian, :640 uniform, :337 file).  Vectors are 3 doubles. */
+srs_status srs_sim_add_bfield_undulator(srs_sim *sim, const double bfield[3], const double period[3],
+                                        int32_t nperiods, double phase, const double rotations[3],
+                                        const double translation[3], double taper);
+srs_status srs_sim_add_bfield_gaussian(srs_sim *sim, const double bfield[3], const double sigma[3],
+                                       const double rotations[3], const double translation[3]);
+srs_status srs_sim_add_bfield_uniform(srs_sim *sim, const double bfield[3], const double width[3],
+                                      const double rotations[3], const double translation[3]);
+/* OSCARS-format field map file (TField3D_Grid::ReadFile): scale[0..2] step scaling, [3..5] field
+ * scaling (nscale may be 0). */
+srs_status srs_sim_add_bfield_file(srs_sim *sim, const char *path, const char *format,
+                                   const double rotations[3], const double translation[3],
+                                   const double *scale, int32_t nscale);
+/* Field map given as arrays (same meaning as the file's header and body). */
+srs_status srs_sim_add_bfield_grid(srs_sim *sim, const double start[3], const double step[3],
+                                   const int64_t n[3], const double *data, const double rotations[3],
+                                   const double translation[3]);
+srs_status srs_sim_clear_bfields(srs_sim *sim);
+int32_t srs_sim_get_nfields(srs_sim *sim);
+/* Field at points (evaluated on the device): xyz and out are HOST arrays of 3*np doubles. */
+srs_status srs_sim_get_bfield(srs_sim *sim, const double *xyz, int64_t np, double *out);
+/* Replace field k's grid samples (DEVICE or HOST pointer, 3*nsamples doubles): used by the adjoint. */
+srs_status srs_sim_set_field_grid_data(srs_sim *sim, int32_t k, const double *data, int32_t on_device);
+
+/* Particle beams (:1661 add_particle_beam; set_particle_beam = clear + add + ideal particle).
+ * hdir/beta/emittance may be NULL (not given); type "custom" uses mass [kg] and charge [C]. */
+typedef struct srs_beam_args {
+  const char *type;
+  const char *name;
+  double energy_gev;
+  double d0[3];
+  double x0[3];
+  double sigma_energy_gev;
+  double t0;
+  double current;
+  double weight;
+  double rotations[3];
+  double translation[3];
+  const double *horizontal_direction; /* 3 or NULL */
+  const double *beta;                 /* 2 or NULL */
+  const double *emittance;            /* 2 or NULL */
+  double lattice_reference[3];
+  double mass;
+  double charge;
+} srs_beam_args;
+srs_status srs_sim_add_particle_beam(srs_sim *sim, const srs_beam_args *args);
+srs_status srs_sim_clear_particle_beams(srs_sim *sim);
+int32_t srs_sim_get_nparticle_beams(srs_sim *sim);
+/* beam "" = chosen by weight; which "ideal", "random" or "" (random). */
+srs_status srs_sim_set_new_particle(srs_sim *sim, const char *beam, const char *which);
+/* Current particle: x0, beta0, E0 [GeV], gamma, q/(m gamma), t0, q, current. */
+srs_status srs_sim_get_particle(srs_sim *sim, double x0[3], double beta0[3], double *e0, double *gamma);
+
+/* Process-wide generator (TRandomA: std::mt19937 + std::normal_distribution<double>). */
+void srs_set_seed(double seed);
+double srs_random_uniform(void);
+double srs_random_normal(void);
+/* Reseed AND forget the normal distribution's cached value: the generator state of a freshly
+ * started process after set_seed(seed).  (srs_set_seed, like the reference's set_seed, keeps it.) */
+void srs_random_reset(double seed);
+
+/* Trajectory of the current particle: first call with x == NULL returns n; then x and beta (HOST,
+ * 3*n doubles each, point-major x,y,z) are filled (OSCARSSR_Python.cc:1988-2037). */
+srs_status srs_sim_calculate_trajectory(srs_sim *sim, int64_t *n, double *x, double *beta);
+
+/* The sums for the current particle (nparticles == 0) or nparticles sampled particles with weight
+ * 1/nparticles; results are Kahan-added into out/comp (HOST, length nout), as the reference's
+ * containers.  For the power density, weighted != 0 applies the weight (the reference's GPU path)
+ * and 0 does not (its CPU paths). */
+srs_status srs_sim_calculate_spectrum(srs_sim *sim, const double obs[3], const double *energies,
+                                      int64_t ne, int32_t nparticles, int32_t precision, double *out,
+                                      double *comp);
+srs_status srs_sim_calculate_flux(srs_sim *sim, const double *points, int64_t np,
+                                  const srs_grid2d *grid, double energy_ev, int32_t nparticles,
+                                  int32_t precision, double *out, double *comp);
+srs_status srs_sim_calculate_power_density(srs_sim *sim, const double *points, const double *normals,
+                                           int64_t np, const srs_grid2d *grid, int32_t directional,
+                                           int32_t nparticles, int32_t weighted, int32_t precision,
+                                           double *out, double *comp);
+srs_status srs_sim_calculate_total_power(srs_sim *sim, double *out);
+
+/* ------------------------------------------------------------------ measurement */
+
+/* Instruction throughput of one pipe of the current device, all SMs, from a timed launch of
+ * independent dependency chains: kind 0 = FP32 FFMA, 1 = FP64 DFMA, 2 = SFU sine (MUFU).
+ * ops_per_s receives instructions per second (an FMA counts as one).  Used as roofline denominators
+ * for the compute-bound sums.  No counterpart in the reference. */
+srs_status srs_measure_peak(int32_t kind, double *ops_per_s, void *stream);
+
+/* ------------------------------------------------------------------ host-side geometry */
+
+/* Spectrum energy grid (TSpectrumContainer::Init, TSpectrumContainer.cc:55-86): e0 + (e1-e0)/(n-1)*(i+1). */
+srs_status srs_energy_grid(int64_t n, double e0, double e1, double *out);
+
+/* Rectangle surfaces (TSurfacePoints_Rectangle.cc).  xyz: 3*n1*n2, x12: 2*n1*n2 (GetX1/GetX2),
+ * normal: the unit normal, grid: the same points as a regular grid (for SRS_PRECISION_MIXED). */
+srs_status srs_rectangle_plane(const char *plane, int32_t n1, int32_t n2, double w1, double w2,
+                               const double rotations[3], const double translation[3], int32_t normal,
+                               double *xyz, double *x12, double nrm[3], srs_grid2d *grid);
+srs_status srs_rectangle_points(int32_t n1, int32_t n2, const double x0[3], const double x1[3],
+                                const double x2[3], const double rotations[3],
+                                const double translation[3], int32_t normal, double *xyz, double *x12,
+                                double nrm[3], srs_grid2d *grid);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,197 @@
+// C ABI of the kernels (include/srs_b200.h): argument checks, stream-ordered scratch, dispatch.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "srs_device.cuh"
+#include "srs_internal.h"
+
+namespace srs {
+
+static thread_local std::string g_error;
+
+void set_error(const std::string &msg) { g_error = msg; }
+void clear_error() { g_error.clear(); }
+srs_status fail(srs_status code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+srs_status cuda_fail(cudaError_t e, const char *what) {
+  g_error = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+  return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? SRS_ERR_NO_DEVICE : SRS_ERR_CUDA;
+}
+
+static srs_status check_view(const srs_traj_view &t, bool need_aoc) {
+  if (!t.x || !t.beta || (need_aoc && !t.aoc)) return fail(SRS_ERR_INVALID, "trajectory pointers are NULL");
+  if (t.n < 1) return fail(SRS_ERR_RANGE, "no points in trajectory.  Is particle or beam defined?");
+  if (t.nparticles < 1) return fail(SRS_ERR_INVALID, "nparticles must be >= 1");
+  if (!(t.dt > 0) || !std::isfinite(t.dt)) return fail(SRS_ERR_INVALID, "trajectory time step must be > 0");
+  return SRS_OK;
+}
+
+}  // namespace srs
+
+using namespace srs;
+
+extern "C" {
+
+const char *srs_last_error(void) { return g_error.c_str(); }
+const char *srs_version(void) { return "srs_b200 1.0.0 (sm_100a)"; }
+
+int srs_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+srs_status srs_trajectory_counts(double ctstart, double ctstop, double t0, int64_t npoints, double *dt,
+                                 int64_t *nforward, int64_t *nbackward) {
+  clear_error();
+  if (ctstart > t0) return fail(SRS_ERR_RANGE, "start time is greater than T0");
+  if (ctstart >= ctstop)
+    return fail(SRS_ERR_RANGE, "start time is greater than stop time.  check that set_ctstartstop is set");
+  if (npoints < 2) return fail(SRS_ERR_RANGE, "npoints_trajectory must be >= 2");
+  // OSCARSSR.cc:592-598, same expressions (size_t truncation included)
+  const double DeltaT = ((ctstop - ctstart) / kC / (double)(size_t)(npoints - 1));
+  const double f = 1 + (ctstop - t0) / kC / DeltaT;
+  const double b = (t0 - ctstart) / kC / DeltaT;
+  if (!(f >= 0) || !(b >= 0) || f > 4e9 || b > 4e9) return fail(SRS_ERR_RANGE, "trajectory point count out of range");
+  if (dt) *dt = DeltaT;
+  if (nforward) *nforward = (int64_t)(size_t)f;
+  if (nbackward) *nbackward = (int64_t)(size_t)b;
+  return SRS_OK;
+}
+
+srs_status srs_trajectory(const srs_field *fields, int32_t nfields, const srs_particle *particles,
+                          int32_t nparticles, double ctstart, double ctstop, double t0, int64_t npoints,
+                          double *d_x, double *d_beta, double *d_aoc, void *stream) {
+  clear_error();
+  double dt;
+  int64_t nf, nb;
+  srs_status st = srs_trajectory_counts(ctstart, ctstop, t0, npoints, &dt, &nf, &nb);
+  if (st) return st;
+  if (nfields < 0 || (nfields > 0 && !fields)) return fail(SRS_ERR_INVALID, "bad field array");
+  if (nparticles < 1 || !particles) return fail(SRS_ERR_INVALID, "bad particle array");
+  if (!d_x || !d_beta || !d_aoc) return fail(SRS_ERR_INVALID, "output pointers are NULL");
+  for (int i = 0; i < nfields; ++i)
+    if (fields[i].kind == SRS_FIELD_GRID && !fields[i].data)
+      return fail(SRS_ERR_INVALID, "grid field without data");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DeviceBuffer df, dp;
+  SRS_CUDA(df.alloc(sizeof(srs_field) * (nfields > 0 ? nfields : 1), s));
+  SRS_CUDA(dp.alloc(sizeof(srs_particle) * nparticles, s));
+  if (nfields > 0) SRS_CUDA(cudaMemcpyAsync(df.ptr, fields, sizeof(srs_field) * nfields, cudaMemcpyHostToDevice, s));
+  SRS_CUDA(cudaMemcpyAsync(dp.ptr, particles, sizeof(srs_particle) * nparticles, cudaMemcpyHostToDevice, s));
+  SRS_CUDA(launch_rk4(df.as<srs_field>(), nfields, dp.as<srs_particle>(), nparticles, dt, nf, nb, d_x, d_beta, d_aoc, s));
+  return SRS_OK;
+}
+
+srs_status srs_spectrum(srs_traj_view traj, srs_beam_consts beam, const double obs[3], const double *d_energies,
+                        int64_t ne, int32_t precision, double *d_out, void *stream) {
+  clear_error();
+  if (srs_status st = check_view(traj, false)) return st;
+  if (!obs || !d_out || (ne > 0 && !d_energies)) return fail(SRS_ERR_INVALID, "NULL argument");
+  if (ne < 1) return fail(SRS_ERR_INVALID, "'npoints' must be > 0");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DeviceBuffer scratch;
+  if (precision == SRS_PRECISION_FP64) {
+    SRS_CUDA(scratch.alloc(fp64_spectrum_scratch_bytes(traj.n, ne, traj.nparticles), s));
+    SRS_CUDA(fp64_spectrum(traj, beam, obs, d_energies, ne, d_out, scratch.ptr, s));
+  } else if (precision == SRS_PRECISION_MIXED) {
+    SRS_CUDA(scratch.alloc(mixed_spectrum_scratch_bytes(traj.n, ne, traj.nparticles), s));
+    SRS_CUDA(mixed_spectrum(traj, beam, obs, d_energies, ne, d_out, scratch.ptr, s));
+  } else {
+    return fail(SRS_ERR_INVALID, "unknown precision");
+  }
+  return SRS_OK;
+}
+
+srs_status srs_flux(srs_traj_view traj, srs_beam_consts beam, const double *d_points, int64_t np,
+                    const srs_grid2d *grid, double energy_ev, int32_t precision, double *d_out, void *stream) {
+  clear_error();
+  if (srs_status st = check_view(traj, false)) return st;
+  if (!d_out) return fail(SRS_ERR_INVALID, "NULL output");
+  if (np < 1) return fail(SRS_ERR_INVALID, "no observation points");
+  if (!(energy_ev > 0)) return fail(SRS_ERR_INVALID, "energy_eV must be > 0");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DeviceBuffer scratch;
+  if (precision == SRS_PRECISION_FP64) {
+    if (!d_points) return fail(SRS_ERR_INVALID, "NULL points");
+    SRS_CUDA(scratch.alloc(fp64_flux_scratch_bytes(traj.n, np, traj.nparticles), s));
+    SRS_CUDA(fp64_flux(traj, beam, d_points, np, energy_ev, d_out, scratch.ptr, s));
+  } else if (precision == SRS_PRECISION_MIXED) {
+    if (!grid) return fail(SRS_ERR_INVALID, "mixed-precision flux needs the points as a regular grid");
+    if ((int64_t)grid->n1 * grid->n2 != np || grid->n1 < 1 || grid->n2 < 1)
+      return fail(SRS_ERR_INVALID, "grid size does not match the number of points");
+    SRS_CUDA(scratch.alloc(mixed_flux_scratch_bytes(traj.n, *grid, traj.nparticles), s));
+    SRS_CUDA(mixed_flux(traj, beam, *grid, energy_ev, d_out, scratch.ptr, s));
+  } else {
+    return fail(SRS_ERR_INVALID, "unknown precision");
+  }
+  return SRS_OK;
+}
+
+srs_status srs_power_density(srs_traj_view traj, srs_beam_consts beam, const double *d_points,
+                             const double *d_normals, int64_t np, const srs_grid2d *grid, int32_t directional,
+                             int32_t precision, double *d_out, void *stream) {
+  clear_error();
+  if (srs_status st = check_view(traj, true)) return st;
+  if (!d_out) return fail(SRS_ERR_INVALID, "NULL output");
+  if (np < 1) return fail(SRS_ERR_INVALID, "no observation points");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DeviceBuffer scratch;
+  if (precision == SRS_PRECISION_FP64) {
+    if (!d_points || !d_normals) return fail(SRS_ERR_INVALID, "NULL points or normals");
+    SRS_CUDA(scratch.alloc(fp64_pd_scratch_bytes(traj.n, np, traj.nparticles), s));
+    SRS_CUDA(fp64_power_density(traj, beam, d_points, d_normals, np, directional, d_out, scratch.ptr, s));
+  } else if (precision == SRS_PRECISION_MIXED) {
+    if (!grid) return fail(SRS_ERR_INVALID, "mixed-precision power density needs the points as a regular grid");
+    if ((int64_t)grid->n1 * grid->n2 != np || grid->n1 < 1 || grid->n2 < 1)
+      return fail(SRS_ERR_INVALID, "grid size does not match the number of points");
+    SRS_CUDA(scratch.alloc(mixed_pd_scratch_bytes(traj.n, *grid, traj.nparticles), s));
+    SRS_CUDA(mixed_power_density(traj, beam, *grid, directional, d_out, scratch.ptr, s));
+  } else {
+    return fail(SRS_ERR_INVALID, "unknown precision");
+  }
+  return SRS_OK;
+}
+
+srs_status srs_total_power(srs_traj_view traj, srs_beam_consts beam, const double *gamma, double *out, void *stream) {
+  clear_error();
+  if (srs_status st = check_view(traj, true)) return st;
+  if (!gamma || !out) return fail(SRS_ERR_INVALID, "NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DeviceBuffer dg, dout;
+  SRS_CUDA(dg.alloc(sizeof(double) * traj.nparticles, s));
+  SRS_CUDA(dout.alloc(sizeof(double) * traj.nparticles, s));
+  SRS_CUDA(cudaMemcpyAsync(dg.ptr, gamma, sizeof(double) * traj.nparticles, cudaMemcpyHostToDevice, s));
+  SRS_CUDA(total_power(traj, beam, dg.as<double>(), dout.as<double>(), s));
+  SRS_CUDA(cudaMemcpyAsync(out, dout.ptr, sizeof(double) * traj.nparticles, cudaMemcpyDeviceToHost, s));
+  SRS_CUDA(cudaStreamSynchronize(s));
+  return SRS_OK;
+}
+
+srs_status srs_accumulate(const double *d_vals, int32_t nparticles, int64_t nout, double weight, double *out,
+                          double *comp, void *stream) {
+  clear_error();
+  if (!d_vals || !out || !comp || nparticles < 1 || nout < 0) return fail(SRS_ERR_INVALID, "bad argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DeviceBuffer dout;
+  SRS_CUDA(dout.alloc(sizeof(double) * 2 * nout, s));
+  double *o = dout.as<double>(), *c = o + nout;
+  SRS_CUDA(cudaMemcpyAsync(o, out, sizeof(double) * nout, cudaMemcpyHostToDevice, s));
+  SRS_CUDA(cudaMemcpyAsync(c, comp, sizeof(double) * nout, cudaMemcpyHostToDevice, s));
+  SRS_CUDA(accumulate_particles(d_vals, nparticles, nout, weight, o, c, s));
+  SRS_CUDA(cudaMemcpyAsync(out, o, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+  SRS_CUDA(cudaMemcpyAsync(comp, c, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+  SRS_CUDA(cudaStreamSynchronize(s));
+  return SRS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,90 @@
+// Internal declarations shared by the library's translation units (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/srs_b200.h"
+
+namespace srs {
+
+// ---- error reporting: a thread-local message behind srs_last_error() ----
+void set_error(const std::string &msg);
+void clear_error();
+srs_status fail(srs_status code, const std::string &msg);
+srs_status cuda_fail(cudaError_t e, const char *what);
+
+#define SRS_CUDA(call)                                              \
+  do {                                                              \
+    cudaError_t srs_e_ = (call);                                    \
+    if (srs_e_ != cudaSuccess) return ::srs::cuda_fail(srs_e_, #call); \
+  } while (0)
+
+// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on the caller's stream).
+struct DeviceBuffer {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer &) = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  ~DeviceBuffer() { release(); }
+  cudaError_t alloc(size_t n, cudaStream_t s) {
+    release();
+    stream = s;
+    bytes = n;
+    if (n == 0) return cudaSuccess;
+    return cudaMallocAsync(&ptr, n, s);
+  }
+  void release() {
+    if (ptr) cudaFreeAsync(ptr, stream);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// ---- kernel launchers ----
+cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
+                       double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
+                       cudaStream_t s);
+cudaError_t launch_field_eval(const srs_field *d_fields, int nfields, const double *d_xyz, int64_t np,
+                              double *d_out, cudaStream_t s);
+
+// Plain FP64 sums.  Scratch is caller-provided (size from the *_scratch_bytes functions).
+size_t fp64_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles);
+cudaError_t fp64_spectrum(const srs_traj_view &t, const srs_beam_consts &b, const double obs[3],
+                          const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s);
+size_t fp64_flux_scratch_bytes(int64_t n, int64_t np, int nparticles);
+cudaError_t fp64_flux(const srs_traj_view &t, const srs_beam_consts &b, const double *d_points, int64_t np,
+                      double energy_ev, double *d_out, void *scratch, cudaStream_t s);
+size_t fp64_pd_scratch_bytes(int64_t n, int64_t np, int nparticles);
+cudaError_t fp64_power_density(const srs_traj_view &t, const srs_beam_consts &b, const double *d_points,
+                               const double *d_normals, int64_t np, int directional, double *d_out, void *scratch,
+                               cudaStream_t s);
+cudaError_t total_power(const srs_traj_view &t, const srs_beam_consts &b, const double *d_gamma, double *d_out,
+                        cudaStream_t s);
+cudaError_t accumulate_particles(const double *d_vals, int nparticles, int64_t nout, double weight, double *d_out,
+                                 double *d_comp, cudaStream_t s);
+
+// Mixed-precision sums.
+size_t mixed_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles);
+cudaError_t mixed_spectrum(const srs_traj_view &t, const srs_beam_consts &b, const double obs[3],
+                           const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s);
+size_t mixed_flux_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles);
+cudaError_t mixed_flux(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g, double energy_ev,
+                       double *d_out, void *scratch, cudaStream_t s);
+size_t mixed_pd_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles);
+cudaError_t mixed_power_density(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g,
+                                int directional, double *d_out, void *scratch, cudaStream_t s);
+
+// Finishing kernels shared by both precisions: add the S per-chunk partial sums in chunk order and
+// apply the reference's final scaling.
+cudaError_t finish_flux_partials(const double *partial, int S, int64_t nout, int nparticles, const double *omegas,
+                                 double omega0, double dt, double C0, double C2, double *out, cudaStream_t s);
+cudaError_t finish_pd_partials(const double *partial, int S, int64_t np, int nparticles, double cdt, int directional,
+                               double *out, cudaStream_t s);
+
+}  // namespace srs

@@ -1,0 +1,437 @@
+// Mixed-precision radiation sums: FP64 only where stability needs it (the retarded phase and its
+// reduction modulo 2*pi, 1 - n.beta, the geometry anchors), FP32 for the bulk of the integrand
+// (amplitude, per-pair phase increments, sincos on the SFU, accumulation), FP64 for the outer sums.
+//
+// Same physics as the plain kernels (src/OSCARSSR.cc:1154-1251 spectrum, :1989-2099 flux,
+// :1477-1598 power density), reorganised for the B200:
+//
+// * Flux / power density on a regular grid of observation points (a rectangle surface): a CTA owns
+//   an 8 x 16 tile of points and one chunk of the trajectory.  For each trajectory point i the CTA
+//   computes ONCE, in FP64, an anchor at the tile's centre point c: distance D_c, direction n_c, the
+//   reduced phase Phi_c = w (t_i + D_c/c) mod 2pi, the reduced per-grid-step phase increments
+//   k1,k2 = (w/c) n_c.u1,u2 mod 2pi, and n_c - beta_hat.  Every point j = c + da*u1 + db*u2 of the
+//   tile then needs only FP32 work on small quantities:
+//       g = n_c . Delta_j,  h = |Delta_j|^2 - g^2,
+//       D_j - D_c = g + h/(2 D_c) (1 - g/D_c) + O(|Delta|^4/D^3),
+//       phase_j = Phi_c + k1 da + k2 db + (w/c) h/(2 D_c) (1 - g/D_c),
+//       n_j - beta_hat = (n_c - beta_hat) + (Delta_j - n_c (D_j - D_c)) / D_j,
+//   so no FP32 quantity is ever the difference of two nearly equal large numbers.
+//   1 - n.beta = (1 - |beta|) + |beta| |n - beta_hat|^2 / 2 (both terms >= 0, no cancellation).
+// * Spectrum on a uniform energy grid: a thread owns 4 consecutive energies; per trajectory point it
+//   forms one FP64 anchor exp(i w_k0 tau_i) and walks the others with the per-point rotation
+//   exp(i dw tau_i) (computed once per point per CTA in FP64), re-anchored at every point.  A
+//   non-uniform grid gets one reduced sincos per (point, energy).
+//
+// Accumulation: FP32 within each 128-point shared-memory tile, then FP64 across tiles and chunks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "srs_device.cuh"
+#include "srs_internal.h"
+
+namespace srs {
+
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kTileA = 8, kTileB = 16;  // points of a CTA tile along u1 and u2 (kTileA * kTileB == kThreads)
+constexpr int kSub = 128;               // trajectory points per shared-memory tile
+constexpr int kTargetCtas = 148 * 6;
+constexpr int kEnergiesPerThread = 4;
+
+int splits_for(int64_t ctas, int64_t n, int64_t min_chunk) {
+  int64_t s = (kTargetCtas + ctas - 1) / std::max<int64_t>(1, ctas);
+  int64_t max_s = std::max<int64_t>(1, n / min_chunk);
+  return (int)std::min<int64_t>(std::max<int64_t>(1, std::min(s, max_s)), 65535);
+}
+
+struct GridTiles {
+  int t1, t2;  // tiles along n1 and n2
+};
+GridTiles tiles_of(const srs_grid2d &g) { return GridTiles{(g.n1 + kTileA - 1) / kTileA, (g.n2 + kTileB - 1) / kTileB}; }
+
+// FP64 anchor common to flux and power density: the tile centre as seen from trajectory point i.
+struct Anchor {
+  double Dc, invDc;
+  double nc[3];
+  double dc[3];   // n_c - beta_hat
+  double bhat[3];
+  double bmag, omb;
+};
+
+__device__ inline Anchor make_anchor(const double Oc[3], const double *xp, const double *bp, int64_t n, int64_t i) {
+  Anchor a;
+  const double rx = Oc[0] - xp[i], ry = Oc[1] - xp[n + i], rz = Oc[2] - xp[2 * n + i];
+  const double d2 = rx * rx + ry * ry + rz * rz;
+  a.Dc = sqrt(d2);
+  a.invDc = 1.0 / a.Dc;
+  a.nc[0] = rx * a.invDc; a.nc[1] = ry * a.invDc; a.nc[2] = rz * a.invDc;
+  const double bx = bp[i], by = bp[n + i], bz = bp[2 * n + i];
+  const double b2 = bx * bx + by * by + bz * bz;
+  a.bmag = sqrt(b2);
+  const double ib = 1.0 / a.bmag;
+  a.bhat[0] = bx * ib; a.bhat[1] = by * ib; a.bhat[2] = bz * ib;
+  a.omb = (1.0 - b2) / (1.0 + a.bmag);  // 1 - |beta|, via 1 - |beta|^2 = 1/gamma^2
+  for (int c = 0; c < 3; ++c) a.dc[c] = a.nc[c] - a.bhat[c];
+  return a;
+}
+
+// ---------------------------------------------------------------- flux on a grid
+
+struct FluxRec {  // per trajectory point, per tile (FP32 unless noted)
+  float phi, k1, k2, w1, invD, D;
+  float nc[3], dc[3], bo[3], bim[3];
+};
+
+__global__ void __launch_bounds__(kThreads) flux_mixed_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
+                                                              int64_t n, double dt, srs_grid2d g, double omega,
+                                                              int64_t chunk, double *__restrict__ partial) {
+  __shared__ float sm[18][kSub];
+  const int tid = threadIdx.x;
+  const int T1 = blockIdx.x / ((g.n2 + kTileB - 1) / kTileB), T2 = blockIdx.x % ((g.n2 + kTileB - 1) / kTileB);
+  const int a = tid / kTileB, b = tid % kTileB;
+  const int i1 = T1 * kTileA + a, i2 = T2 * kTileB + b;
+  const bool active = i1 < g.n1 && i2 < g.n2;
+  const int64_t j = (int64_t)i1 * g.n2 + i2;
+  const int64_t np = (int64_t)g.n1 * g.n2;
+  const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
+  const double *xp = X + (int64_t)p * 3 * n, *bp = Bt + (int64_t)p * 3 * n;
+  const int64_t i0 = (int64_t)s * chunk, iend = imin64(n, i0 + chunk);
+  // tile centre (a grid point) and this thread's integer offsets from it
+  const int ca = T1 * kTileA + kTileA / 2, cb = T2 * kTileB + kTileB / 2;
+  double Oc[3];
+  for (int c = 0; c < 3; ++c) Oc[c] = g.origin[c] + (double)ca * g.u1[c] + (double)cb * g.u2[c];
+  const int da = i1 - ca, db = i2 - cb;
+  float Dl[3];
+  for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);
+  const float dd = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
+  const float fda = (float)da, fdb = (float)db;
+  const double wc = omega / kC;
+  const float cow = (float)(kC / omega);
+  double E[6] = {0, 0, 0, 0, 0, 0};
+
+  for (int64_t base = i0; base < iend; base += kSub) {
+    const int cnt = (int)imin64(kSub, iend - base);
+    __syncthreads();
+    if (tid < cnt) {
+      const int64_t i = base + tid;
+      const Anchor A = make_anchor(Oc, xp, bp, n, i);
+      const double tau = dt * (double)i + A.Dc / kC;
+      sm[0][tid] = (float)reduce_2pi(omega * tau);
+      sm[1][tid] = (float)reduce_2pi(wc * (A.nc[0] * g.u1[0] + A.nc[1] * g.u1[1] + A.nc[2] * g.u1[2]));
+      sm[2][tid] = (float)reduce_2pi(wc * (A.nc[0] * g.u2[0] + A.nc[1] * g.u2[1] + A.nc[2] * g.u2[2]));
+      sm[3][tid] = (float)(wc * 0.5 * A.invDc);
+      sm[4][tid] = (float)A.invDc;
+      sm[5][tid] = (float)A.Dc;
+      const double bimc = -(kC / omega) * A.invDc * A.invDc;  // near-field term -i (c/w) n / D^2 at the centre
+      for (int c = 0; c < 3; ++c) {
+        sm[6 + c][tid] = (float)A.nc[c];
+        sm[9 + c][tid] = (float)A.dc[c];
+        sm[12 + c][tid] = (float)(A.bhat[c] * A.omb);
+        sm[15 + c][tid] = (float)(bimc * A.nc[c]);
+      }
+    }
+    __syncthreads();
+    if (!active) continue;
+    float e0 = 0, e1 = 0, e2 = 0, e3 = 0, e4 = 0, e5 = 0;
+#pragma unroll 4
+    for (int k = 0; k < cnt; ++k) {
+      const float ncx = sm[6][k], ncy = sm[7][k], ncz = sm[8][k];
+      const float gq = fmaf(ncz, Dl[2], fmaf(ncy, Dl[1], ncx * Dl[0]));
+      const float h = fmaf(-gq, gq, dd);
+      const float invD = sm[4][k];
+      const float q = h * sm[3][k] * fmaf(-gq, invD, 1.0f);      // (w/c)(D_j - D_c - g)
+      const float del = fmaf(q, cow, gq);                          // D_j - D_c
+      const float rinv = __fdividef(1.0f, sm[5][k] + del);
+      float ph = fmaf(sm[1][k], fda, sm[0][k]);
+      ph = fmaf(sm[2][k], fdb, ph) + q;
+      float sn, cs;
+      __sincosf(reduce_2pi_f(ph), &sn, &cs);
+      // amplitude (beta - n_j)/D_j = -((n_j - bhat) + bhat*omb)/D_j
+      const float dnx = fmaf(-ncx, del, Dl[0]) * rinv, dny = fmaf(-ncy, del, Dl[1]) * rinv, dnz = fmaf(-ncz, del, Dl[2]) * rinv;
+      const float ax = -(sm[9][k] + dnx + sm[12][k]) * rinv;
+      const float ay = -(sm[10][k] + dny + sm[13][k]) * rinv;
+      const float az = -(sm[11][k] + dnz + sm[14][k]) * rinv;
+      const float bx = sm[15][k], by = sm[16][k], bz = sm[17][k];
+      e0 = fmaf(ax, cs, fmaf(-bx, sn, e0)); e1 = fmaf(ax, sn, fmaf(bx, cs, e1));
+      e2 = fmaf(ay, cs, fmaf(-by, sn, e2)); e3 = fmaf(ay, sn, fmaf(by, cs, e3));
+      e4 = fmaf(az, cs, fmaf(-bz, sn, e4)); e5 = fmaf(az, sn, fmaf(bz, cs, e5));
+    }
+    E[0] += e0; E[1] += e1; E[2] += e2; E[3] += e3; E[4] += e4; E[5] += e5;
+  }
+  if (active) {
+    double *o = partial + ((int64_t)p * S + s) * 6 * np + j;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) o[c * np] = E[c];
+  }
+}
+
+// ---------------------------------------------------------------- power density on a grid
+
+__global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
+                                                            const double *__restrict__ Ac, int64_t n, srs_grid2d g,
+                                                            double nx_, double ny_, double nz_, int directional,
+                                                            int64_t chunk, double *__restrict__ partial) {
+  __shared__ float sm[17][kSub];
+  const int tid = threadIdx.x;
+  const int nt2 = (g.n2 + kTileB - 1) / kTileB;
+  const int T1 = blockIdx.x / nt2, T2 = blockIdx.x % nt2;
+  const int a = tid / kTileB, b = tid % kTileB;
+  const int i1 = T1 * kTileA + a, i2 = T2 * kTileB + b;
+  const bool active = i1 < g.n1 && i2 < g.n2;
+  const int64_t j = (int64_t)i1 * g.n2 + i2;
+  const int64_t np = (int64_t)g.n1 * g.n2;
+  const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
+  const int64_t off = (int64_t)p * 3 * n;
+  const double *xp = X + off, *bp = Bt + off, *ap = Ac + off;
+  const int64_t i0 = (int64_t)s * chunk, iend = imin64(n, i0 + chunk);
+  const int ca = T1 * kTileA + kTileA / 2, cb = T2 * kTileB + kTileB / 2;
+  double Oc[3];
+  for (int c = 0; c < 3; ++c) Oc[c] = g.origin[c] + (double)ca * g.u1[c] + (double)cb * g.u2[c];
+  const int da = i1 - ca, db = i2 - cb;
+  float Dl[3];
+  for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);
+  const float dd = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
+  const float nrx = (float)nx_, nry = (float)ny_, nrz = (float)nz_;
+  double sum = 0;
+  for (int64_t base = i0; base < iend; base += kSub) {
+    const int cnt = (int)imin64(kSub, iend - base);
+    __syncthreads();
+    if (tid < cnt) {
+      const int64_t i = base + tid;
+      const Anchor A = make_anchor(Oc, xp, bp, n, i);
+      const double ax = ap[i], ay = ap[n + i], az = ap[2 * n + i];
+      sm[0][tid] = (float)A.invDc;
+      sm[1][tid] = (float)A.Dc;
+      sm[2][tid] = (float)A.omb;
+      sm[3][tid] = (float)(0.5 * A.bmag);
+      sm[4][tid] = (float)(A.bhat[0] * ax + A.bhat[1] * ay + A.bhat[2] * az);  // bhat . a
+      for (int c = 0; c < 3; ++c) {
+        sm[5 + c][tid] = (float)A.nc[c];
+        sm[8 + c][tid] = (float)A.dc[c];
+        sm[11 + c][tid] = (float)(A.bhat[c] * A.omb);
+      }
+      sm[14][tid] = (float)ax; sm[15][tid] = (float)ay; sm[16][tid] = (float)az;
+    }
+    __syncthreads();
+    if (!active) continue;
+    float acc = 0;
+#pragma unroll 4
+    for (int k = 0; k < cnt; ++k) {
+      const float ncx = sm[5][k], ncy = sm[6][k], ncz = sm[7][k];
+      const float gq = fmaf(ncz, Dl[2], fmaf(ncy, Dl[1], ncx * Dl[0]));
+      const float h = fmaf(-gq, gq, dd);
+      const float invD = sm[0][k];
+      const float del = fmaf(0.5f * h * invD, fmaf(-gq, invD, 1.0f), gq);  // D_j - D_c
+      const float rinv = __fdividef(1.0f, sm[1][k] + del);
+      const float dnx = fmaf(-ncx, del, Dl[0]) * rinv, dny = fmaf(-ncy, del, Dl[1]) * rinv, dnz = fmaf(-ncz, del, Dl[2]) * rinv;
+      const float dx = sm[8][k] + dnx, dy = sm[9][k] + dny, dz = sm[10][k] + dnz;  // n_j - bhat
+      const float nx = ncx + dnx, ny = ncy + dny, nz = ncz + dnz;
+      const float nd = fmaf(nz, nrz, fmaf(ny, nry, nx * nrx));
+      if (directional && nd <= 0.0f) continue;
+      const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      const float opnb = fmaf(sm[3][k], d2, sm[2][k]);  // 1 - n.beta
+      const float axx = sm[14][k], ayy = sm[15][k], azz = sm[16][k];
+      const float na = fmaf(dz, azz, fmaf(dy, ayy, fmaf(dx, axx, sm[4][k])));  // n . a
+      // V = n x ((n - beta) x a) = (n - beta)(n.a) - a (1 - n.beta)
+      const float Xx = dx + sm[11][k], Xy = dy + sm[12][k], Xz = dz + sm[13][k];
+      const float Vx = fmaf(Xx, na, -axx * opnb), Vy = fmaf(Xy, na, -ayy * opnb), Vz = fmaf(Xz, na, -azz * opnb);
+      const float v2 = fmaf(Vz, Vz, fmaf(Vy, Vy, Vx * Vx));
+      const float o2 = opnb * opnb;
+      const float o5 = o2 * o2 * opnb;
+      acc = fmaf(v2 * rinv * rinv * nd, __fdividef(1.0f, o5), acc);
+    }
+    sum += (double)acc;
+  }
+  if (active) partial[((int64_t)p * S + s) * np + j] = sum;
+}
+
+// ---------------------------------------------------------------- spectrum at one observer
+
+// Each thread owns kEnergiesPerThread consecutive energies.  The rotation exp(i dw tau_i) is shared by
+// all threads (dw = (w_last - w_first)/(ne - 1), computed once per trajectory point per CTA); a thread
+// whose energies are not on that uniform grid (|w_k - (w_0 + k dw)| * tau_max > 1e-3 rad) takes one
+// reduced sincos per (point, energy) instead.  No host synchronisation is needed to decide.
+__global__ void __launch_bounds__(kThreads) spectrum_mixed_kernel(const double *__restrict__ X,
+                                                                  const double *__restrict__ Bt, int64_t n, double dt,
+                                                                  V3 obs, const double *__restrict__ omegas, int64_t ne,
+                                                                  int64_t chunk, double *__restrict__ partial) {
+  __shared__ double stau[kSub];
+  __shared__ float sv[8][kSub];  // a = (beta - n)/D (3), b' = n/D^2 (3), rotation exp(i dw tau) (2)
+  constexpr int K = kEnergiesPerThread;
+  const int tid = threadIdx.x;
+  const int64_t k0 = ((int64_t)blockIdx.x * kThreads + tid) * K;
+  const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
+  const double *xp = X + (int64_t)p * 3 * n, *bp = Bt + (int64_t)p * 3 * n;
+  const int64_t i0 = (int64_t)s * chunk, iend = imin64(n, i0 + chunk);
+  const bool active = k0 < ne;
+  const double wfirst = omegas[0];
+  const double dw = ne > 1 ? (omegas[ne - 1] - wfirst) / (double)(ne - 1) : 0.0;
+  float kap[K];  // -c/w_k: the near-field term is i*kap*n/D^2
+  double wk[K];
+  bool uniform = ne > 1;
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    const int64_t k = imin64(k0 + q, ne - 1);
+    wk[q] = omegas[k];
+    kap[q] = (float)(-kC / wk[q]);
+    const double dev = fabs(wk[q] - (wfirst + (double)k * dw));
+    if (k0 + q < ne && dev * (1e3 / kC) >= 1e-3) uniform = false;  // observers within 1 km
+  }
+  double E[K][6];
+#pragma unroll
+  for (int q = 0; q < K; ++q)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) E[q][c] = 0;
+
+  for (int64_t base = i0; base < iend; base += kSub) {
+    const int cnt = (int)imin64(kSub, iend - base);
+    __syncthreads();
+    if (tid < cnt) {
+      const int64_t i = base + tid;
+      const double rx = obs.x - xp[i], ry = obs.y - xp[n + i], rz = obs.z - xp[2 * n + i];
+      const double D = sqrt(rx * rx + ry * ry + rz * rz), iD = 1.0 / D;
+      const double nx = rx * iD, ny = ry * iD, nz = rz * iD;
+      const double tau = dt * (double)i + D / kC;
+      stau[tid] = tau;
+      sv[0][tid] = (float)((bp[i] - nx) * iD);
+      sv[1][tid] = (float)((bp[n + i] - ny) * iD);
+      sv[2][tid] = (float)((bp[2 * n + i] - nz) * iD);
+      const double iD2 = iD * iD;
+      sv[3][tid] = (float)(nx * iD2);
+      sv[4][tid] = (float)(ny * iD2);
+      sv[5][tid] = (float)(nz * iD2);
+      double sr, cr;
+      sincos(reduce_2pi(dw * tau), &sr, &cr);
+      sv[6][tid] = (float)cr;
+      sv[7][tid] = (float)sr;
+    }
+    __syncthreads();
+    if (!active) continue;
+    float e[K][6];
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) e[q][c] = 0;
+    for (int k = 0; k < cnt; ++k) {
+      const double tau = stau[k];
+      const float ax = sv[0][k], ay = sv[1][k], az = sv[2][k];
+      const float bx = sv[3][k], by = sv[4][k], bz = sv[5][k];
+      const float rr = sv[6][k], ri = sv[7][k];
+      float zr, zi;
+      __sincosf((float)reduce_2pi(wk[0] * tau), &zi, &zr);
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        if (q > 0) {
+          if (uniform) {  // z <- z * exp(i dw tau)
+            const float tr = zr * rr - zi * ri;
+            zi = fmaf(zr, ri, zi * rr);
+            zr = tr;
+          } else {
+            __sincosf((float)reduce_2pi(wk[q] * tau), &zi, &zr);
+          }
+        }
+        // e += (a + i kap b') (zr + i zi)
+        const float cx = kap[q] * bx, cy = kap[q] * by, cz = kap[q] * bz;
+        e[q][0] = fmaf(ax, zr, fmaf(-cx, zi, e[q][0])); e[q][1] = fmaf(ax, zi, fmaf(cx, zr, e[q][1]));
+        e[q][2] = fmaf(ay, zr, fmaf(-cy, zi, e[q][2])); e[q][3] = fmaf(ay, zi, fmaf(cy, zr, e[q][3]));
+        e[q][4] = fmaf(az, zr, fmaf(-cz, zi, e[q][4])); e[q][5] = fmaf(az, zi, fmaf(cz, zr, e[q][5]));
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) E[q][c] += (double)e[q][c];
+  }
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      const int64_t k = k0 + q;
+      if (k >= ne) break;
+      double *o = partial + ((int64_t)p * S + s) * 6 * ne + k;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) o[c * ne] = E[q][c];
+    }
+  }
+}
+
+__global__ void omega_kernel(const double *__restrict__ e, int64_t ne, double *__restrict__ w) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ne) w[i] = ev_to_omega(e[i]);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+
+static int flux_mixed_splits(int64_t n, const srs_grid2d &g, int nparticles) {
+  GridTiles t = tiles_of(g);
+  return splits_for((int64_t)t.t1 * t.t2 * nparticles, n, 512);
+}
+
+size_t mixed_flux_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles) {
+  return sizeof(double) * 6 * (size_t)g.n1 * g.n2 * nparticles * flux_mixed_splits(n, g, nparticles);
+}
+
+cudaError_t mixed_flux(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g, double energy_ev,
+                       double *d_out, void *scratch, cudaStream_t s) {
+  const int S = flux_mixed_splits(t.n, g, t.nparticles);
+  const int64_t chunk = (t.n + S - 1) / S;
+  GridTiles tl = tiles_of(g);
+  const double omega = ev_to_omega(energy_ev);
+  double *partial = static_cast<double *>(scratch);
+  dim3 grid((unsigned)(tl.t1 * tl.t2), S, t.nparticles);
+  flux_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt, g, omega, chunk, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return finish_flux_partials(partial, S, (int64_t)g.n1 * g.n2, t.nparticles, nullptr, omega, t.dt, flux_c0(b.charge),
+                              flux_c2(b.charge, b.current), d_out, s);
+}
+
+size_t mixed_pd_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles) {
+  GridTiles tl = tiles_of(g);
+  return sizeof(double) * (size_t)g.n1 * g.n2 * nparticles *
+         splits_for((int64_t)tl.t1 * tl.t2 * nparticles, n, 512);
+}
+
+cudaError_t mixed_power_density(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g,
+                                int directional, double *d_out, void *scratch, cudaStream_t s) {
+  GridTiles tl = tiles_of(g);
+  const int S = splits_for((int64_t)tl.t1 * tl.t2 * t.nparticles, t.n, 512);
+  const int64_t chunk = (t.n + S - 1) / S;
+  double *partial = static_cast<double *>(scratch);
+  dim3 grid((unsigned)(tl.t1 * tl.t2), S, t.nparticles);
+  pd_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.aoc, t.n, g, g.normal[0], g.normal[1], g.normal[2], directional, chunk,
+                                            partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return finish_pd_partials(partial, S, (int64_t)g.n1 * g.n2, t.nparticles, pd_const(b.charge, b.current) * t.dt,
+                            directional, d_out, s);
+}
+
+size_t mixed_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles) {
+  const int64_t ctas = (ne + kThreads * kEnergiesPerThread - 1) / (kThreads * kEnergiesPerThread) * nparticles;
+  return sizeof(double) * ((size_t)6 * ne * nparticles * splits_for(ctas, n, 256) + ne);
+}
+
+cudaError_t mixed_spectrum(const srs_traj_view &t, const srs_beam_consts &b, const double obs[3],
+                           const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s) {
+  const int64_t etiles = (ne + kThreads * kEnergiesPerThread - 1) / (kThreads * kEnergiesPerThread);
+  const int S = splits_for(etiles * t.nparticles, t.n, 256);
+  const int64_t chunk = (t.n + S - 1) / S;
+  double *partial = static_cast<double *>(scratch);
+  double *omegas = partial + (size_t)6 * ne * t.nparticles * S;
+  omega_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(d_energies, ne, omegas);
+  dim3 grid((unsigned)etiles, S, t.nparticles);
+  spectrum_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt, v3(obs[0], obs[1], obs[2]), omegas, ne,
+                                                  chunk, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return finish_flux_partials(partial, S, ne, t.nparticles, omegas, 0.0, t.dt, flux_c0(b.charge),
+                              flux_c2(b.charge, b.current), d_out, s);
+}
+
+}  // namespace srs

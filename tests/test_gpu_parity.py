@@ -1,0 +1,349 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's own outputs (golden fixtures
+made by running the reference) and against the oracle on seeded random inputs.
+
+Tolerances (stated per test):
+  * trajectory (FP64 RK4, reference operation order): relative 1e-12 per component scale;
+  * plain FP64 sums vs the reference CPU path: relative 1e-10, taken as the max over outputs with
+    value >= 1e-6 of the maximum (near exact nulls the relative error is ill-conditioned), plus the
+    normwise error ||a-b||/||b|| <= 1e-12;
+  * mixed-precision sums vs the same reference: max relative error 1e-4 over outputs >= 1e-3 of the
+    maximum, normwise 1e-5.
+"""
+import ctypes as C
+import json
+import math
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import ROOT, golden
+from srsoriginal_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64, TOL_FP64_NORM = 1e-10, 1e-12
+TOL_MIXED, TOL_MIXED_NORM = 1e-4, 1e-5
+
+
+def rel_err(a, b, floor):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    big = np.abs(b) >= floor * np.abs(b).max()
+    mx = float(np.max(np.abs(a[big] - b[big]) / np.abs(b[big])))
+    nrm = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    return mx, nrm
+
+
+def assert_fp64(a, b):
+    mx, nrm = rel_err(a, b, 1e-6)
+    assert mx <= TOL_FP64 and nrm <= TOL_FP64_NORM, (mx, nrm)
+
+
+def assert_mixed(a, b):
+    mx, nrm = rel_err(a, b, 1e-3)
+    assert mx <= TOL_MIXED and nrm <= TOL_MIXED_NORM, (mx, nrm)
+
+
+def new_sr(npoints=20001, fields="undulator", **beam):
+    from srsoriginal_b200.sr import sr
+    o = sr()
+    W.setup_beam(o, npoints, **beam)
+    if fields == "undulator":
+        W.setup_undulator(o)
+    elif fields == "epu":
+        W.setup_epu(o)
+    return o
+
+
+def traj_close(X, ref, tol=1e-12):
+    scale = np.maximum(np.abs(ref).max(axis=1, keepdims=True), 1e-300)
+    return float(np.max(np.abs(X - ref) / scale)) <= tol
+
+
+# ------------------------------------------------------------------ trajectory
+
+def test_trajectory_cfg0_matches_reference():
+    g = golden("spectrum_cfg0.npz")
+    o = new_sr(2001)
+    x, b = o._trajectory_arrays()
+    assert traj_close(x.T, g["small_x"]) and traj_close(b.T, g["small_beta"])
+    o = new_sr(20001)
+    x, b = o._trajectory_arrays()
+    assert x.shape[0] == int(g["n"])
+    assert traj_close(x.T[:, ::50], g["x_sub"]) and traj_close(b.T[:, ::50], g["beta_sub"])
+    lst = o.calculate_trajectory()
+    assert len(lst) == 20001 and len(lst[0]) == 2 and len(lst[0][0]) == 3
+
+
+def test_total_power_matches_reference():
+    g = golden("spectrum_cfg0.npz")
+    assert abs(new_sr(20001).calculate_total_power() / float(g["total_power"]) - 1) < 1e-12
+    g2 = golden("pd_cfg2.npz")
+    assert abs(new_sr(40001, "epu").calculate_total_power() / float(g2["total_power"]) - 1) < 1e-12
+
+
+# ------------------------------------------------------------------ plain FP64 sums (the drop-in)
+
+def test_spectrum_cfg0_fp64_matches_reference():
+    g = golden("spectrum_cfg0.npz")
+    o = new_sr(20001)
+    s = np.array(o.calculate_spectrum(obs=[0, 0, 30], npoints=1000, energy_range_eV=[100, 1000]))
+    assert np.array_equal(s[:, 0], g["energies"])
+    assert_fp64(s[:, 1], g["flux"])
+
+
+def test_flux_cfg1_fp64_matches_reference():
+    g = golden("flux_cfg1.npz")
+    o = new_sr(20001)
+    for tag in ("e1", "e3"):
+        m = o.calculate_flux_rectangle(plane="XY", energy_eV=float(g["energy_" + tag]), width=[0.01, 0.01],
+                                       npoints=[101, 101], translation=[0, 0, 30])
+        assert len(m) == 101 * 101  # default nthreads (threads path): one entry per point
+        v = np.array([p[1] for p in m])
+        assert np.array_equal(np.array([p[0][:2] for p in m]), g["x12"])
+        assert_fp64(v, g["flux_" + tag])
+
+
+def test_power_density_cfg2_fp64_matches_reference():
+    g = golden("pd_cfg2.npz")
+    o = new_sr(40001, "epu")
+    m = o.calculate_power_density_rectangle(plane="XY", width=[0.04, 0.04], npoints=[201, 201],
+                                            translation=[0, 0, 30])
+    assert len(m) == int(g["nlist"])  # threads path lists the points twice (reference quirk)
+    v = np.array([p[1] for p in m])[:201 * 201]
+    assert_fp64(v, g["pd"])
+
+
+def test_misc_fields_surfaces_directional_fp64():
+    from srsoriginal_b200.sr import sr
+    g = golden("misc_fields.npz")
+    o = sr()
+    W.setup_beam(o, 3001)
+    o.add_bfield_undulator(bfield=[0, 0.8, 0.05], period=[0, 0, 0.05], nperiods=11, phase=0.3,
+                           rotations=[0.001, -0.002, 0.3], translation=[0.0001, 0, 0.05], taper=0.01)
+    o.add_bfield_gaussian(bfield=[0.02, 0.3, 0], sigma=[0, 0, 0.05], translation=[0, 0, -0.5],
+                          rotations=[0, 0.01, 0])
+    o.add_bfield_uniform(bfield=[0.0, -0.01, 0.001], width=[0, 0, 0.2], translation=[0, 0, 0.5],
+                         rotations=[0.02, 0, 0])
+    bf = np.array([o.get_bfield([0.0001 * i, -0.0002 * i, -1 + 0.1 * i]) for i in range(21)])
+    assert np.allclose(bf, g["bfield"], rtol=1e-15, atol=1e-300)
+    x, b = o._trajectory_arrays()
+    assert traj_close(x.T, g["x"]) and traj_close(b.T, g["beta"])
+    s = np.array(o.calculate_spectrum(obs=[0.001, -0.0005, 20], npoints=40, energy_range_eV=[50, 2000], nthreads=1))
+    assert_fp64(s[:, 1], g["flux"])
+    s = np.array(o.calculate_spectrum(obs=[0, 0, 25], points_eV=[75.0, 133.3, 401.0, 999.9], nthreads=1))
+    assert_fp64(s[:, 1], g["pts_flux"])
+    p = o.calculate_power_density_rectangle(plane="YZ", width=[0.02, 0.03], npoints=[7, 9],
+                                            rotations=[0, -math.pi / 2, 0], translation=[0.001, 0, 20], normal=1,
+                                            nthreads=1)
+    assert_fp64([q[1] for q in p], g["pd_dir"])
+    assert np.array_equal(np.array([q[0] for q in p]), g["pd_dir_xyz"])
+    p = o.calculate_power_density_rectangle(plane="YZ", width=[0.02, 0.03], npoints=[7, 9],
+                                            rotations=[0, -math.pi / 2, 0], translation=[0.001, 0, 20], normal=-1,
+                                            nthreads=1)
+    assert_fp64([q[1] for q in p], g["pd_neg"])
+    f = o.calculate_flux_rectangle(energy_eV=300.0, npoints=[6, 5], x0x1x2=[[-0.004, -0.003, 25],
+                                                                           [0.004, -0.003, 25],
+                                                                           [-0.004, 0.003, 25.1]],
+                                   nthreads=1, dim=3)
+    assert len(f) == int(g["flux_x0x1x2_len"])
+    assert_fp64([q[1] for q in f][:30], g["flux_x0x1x2"])
+    assert abs(o.calculate_total_power() / float(g["total_power"]) - 1) < 1e-12
+
+
+def test_beam_sampling_and_multiparticle_match_reference():
+    """Replays the fixture's history in one generator state: Twiss-sampled particles after set_seed(0)
+    (bit-identical draws), then nparticles > 0 sums (weighted 1/N and Kahan-summed in particle order;
+    the power density's CPU paths add without weight), then plain draws after set_seed(7.9).  A reseed
+    keeps the normal distribution's cached value, as the reference's does."""
+    from srsoriginal_b200.sr import reset_random
+    g = golden("beam_3a.npz")
+    o = new_sr(2001, **W.BEAM_3A)
+    reset_random(0)  # a fresh process's generator after set_seed(0)
+    xs = []
+    for _ in range(33):
+        o.set_new_particle(particle="random")
+        xs.append(o.get_particle_x0() + o.get_particle_beta0())
+    assert np.array_equal(np.array(xs), np.concatenate([g["x0"], g["beta0"]], axis=1))
+    o.set_seed(0)
+    s = np.array(o.calculate_spectrum(obs=[0, 0, 30], npoints=48, energy_range_eV=[100, 1000], nparticles=4,
+                                      nthreads=1))
+    assert_fp64(s[:, 1], g["flux"])
+    o.set_seed(0)
+    f = o.calculate_flux_rectangle(plane="XY", energy_eV=W.E1_EV, width=[0.01, 0.01], npoints=[5, 5],
+                                   translation=[0, 0, 30], nparticles=3, nthreads=1)
+    assert len(f) == int(g["flux_map_len"])
+    assert_fp64([q[1] for q in f][:25], g["flux_map"][:25])
+    o.set_seed(0)
+    p = o.calculate_power_density_rectangle(plane="XY", width=[0.04, 0.04], npoints=[5, 5],
+                                            translation=[0, 0, 30], nparticles=3, nthreads=1)
+    assert len(p) == int(g["pd_map_len"])
+    assert_fp64([q[1] for q in p][:25], g["pd_map"][:25])
+    o.set_seed(7.9)
+    u = [o.rand() for _ in range(5)] + [o.norm() for _ in range(5)]
+    assert np.array_equal(np.array(u), g["draws"])
+
+
+def test_grid_field_file_cfg4():
+    g = golden("grid_cfg4.npz")
+    from srsoriginal_b200.sr import sr
+    z, by = W.config4_grid()
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "cfg4.txt")
+        W.write_oscars_grid(path, z, by)
+        o = sr()
+        W.setup_beam(o, 20001)
+        o.add_bfield_file(ifile=path, iformat="OSCARS")
+    bf = np.array([o.get_bfield([0, 0, -0.9 + 0.0123 * i]) for i in range(150)])
+    assert np.allclose(bf, g["bfield"], rtol=1e-15, atol=0)
+    x, b = o._trajectory_arrays()
+    assert traj_close(x.T[:, ::50], g["x_sub"])
+    s = np.array(o.calculate_spectrum(obs=[0, 0, 30], npoints=200, energy_range_eV=[0.98 * W.E3_EV, 1.02 * W.E3_EV]))
+    assert_fp64(s[:, 1], g["flux"])
+
+
+def test_dispatch_list_shapes_match_reference():
+    q = json.load(open(os.path.join(ROOT, "tests", "golden", "quirks.json")))
+    for nthreads in (1, 2):
+        o = new_sr(501)
+        f = o.calculate_flux_rectangle(plane="XY", energy_eV=150.0, width=[0.01, 0.01], npoints=[3, 4],
+                                       translation=[0, 0, 30], nthreads=nthreads)
+        p = o.calculate_power_density_rectangle(plane="XY", width=[0.01, 0.01], npoints=[3, 4],
+                                                translation=[0, 0, 30], nthreads=nthreads)
+        p3 = o.calculate_power_density_rectangle(plane="XY", width=[0.01, 0.01], npoints=[3, 4],
+                                                 translation=[0, 0, 30], nthreads=nthreads, dim=3)
+        assert len(f) == q[f"flux_len_nthreads{nthreads}"]
+        assert len(p) == q[f"pd_len_nthreads{nthreads}"]
+        assert p3[0][0] == q[f"pd_dim3_first_nthreads{nthreads}"]
+        assert [c[0] for c in f] == q[f"flux_coords_nthreads{nthreads}"]
+    # gpu=1 path: 2N entries, the second half with x,y,z coordinates
+    o = new_sr(501)
+    f = o.calculate_flux_rectangle(plane="XY", energy_eV=150.0, width=[0.01, 0.01], npoints=[3, 4],
+                                   translation=[0, 0, 30], gpu=1)
+    assert len(f) == 24 and f[12][0][2] == 30.0
+    with pytest.raises(ValueError, match="gpu is 1 and nthreads > 0"):
+        o.calculate_spectrum(obs=[0, 0, 30], npoints=3, energy_range_eV=[100, 200], gpu=1, nthreads=2)
+    with pytest.raises(ValueError, match="'gpu' must be 0 or 1"):
+        o.calculate_spectrum(obs=[0, 0, 30], npoints=3, energy_range_eV=[100, 200], gpu=2)
+
+
+# ------------------------------------------------------------------ C ABI against the oracle, random inputs
+
+def _dev(a):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+
+
+def _vp(t):
+    return C.c_void_p(t.data_ptr())
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_c_abi_random_fields_and_points_vs_oracle(seed):
+    """srs_trajectory / srs_spectrum / srs_flux / srs_power_density called directly with device buffers,
+    on seeded random field layouts and observation points, against the oracle."""
+    import torch
+    from srsoriginal_b200 import _lib
+    L = _lib.lib
+    rng = np.random.default_rng(seed)
+    ofl = [O.undulator([0, rng.uniform(0.3, 1.2), rng.uniform(-0.1, 0.1)], [0, 0, rng.uniform(0.02, 0.08)],
+                       int(rng.integers(3, 15)), phase=rng.uniform(-1, 1),
+                       rotations=rng.uniform(-0.01, 0.01, 3), translation=[0, 0, rng.uniform(-0.1, 0.1)]),
+           O.gaussian([rng.uniform(-0.2, 0.2), 0.1, 0], [0, 0, 0.1], translation=[0, 0, -0.4])]
+    fl = (_lib.Field * 2)()
+    for k, f in enumerate(ofl):
+        for name, _ in _lib.Field._fields_:
+            if name != "data":
+                setattr(fl[k], name, getattr(f, name))
+    x0 = [rng.uniform(-1e-4, 1e-4), rng.uniform(-1e-4, 1e-4), -1.0]
+    bm = O.Beam(energy_GeV=rng.uniform(1.5, 3.5), x0=x0, d0=[rng.uniform(-1e-4, 1e-4), 0, 1], current=0.4)
+    px0, pb0, gam, qomg = bm.particle(False)
+    npts = int(rng.integers(500, 3000))
+    X, Bv, A, dt = O.trajectory(ofl, px0, pb0, qomg, 0.0, 2.0, 0.0, npts)
+    n = X.shape[1]
+    part = _lib.Particle()
+    part.x0 = _lib.v3(px0)
+    part.beta0 = _lib.v3(pb0)
+    part.qomg = qomg
+    dx, db, da = (torch.empty(3 * n, dtype=torch.float64, device="cuda") for _ in range(3))
+    _lib.check(L.srs_trajectory(fl, 2, C.byref(part), 1, 0.0, 2.0, 0.0, npts, _vp(dx), _vp(db), _vp(da), None))
+    torch.cuda.synchronize()
+    assert traj_close(dx.cpu().numpy().reshape(3, n), X) and traj_close(db.cpu().numpy().reshape(3, n), Bv)
+    view = _lib.TrajView(C.cast(dx.data_ptr(), _lib._D), C.cast(db.data_ptr(), _lib._D),
+                         C.cast(da.data_ptr(), _lib._D), n, 1, dt)
+    beam = _lib.BeamConsts(bm.b.q, bm.b.current)
+    # spectrum at a random observer
+    obs = [rng.uniform(-1e-3, 1e-3), rng.uniform(-1e-3, 1e-3), rng.uniform(10, 40)]
+    e = np.sort(rng.uniform(50, 3000, 37))
+    de, out = _dev(e), torch.empty(37, dtype=torch.float64, device="cuda")
+    _lib.check(L.srs_spectrum(view, beam, _lib.v3(obs), _vp(de), 37, _lib.FP64, _vp(out), None))
+    assert_fp64(out.cpu().numpy(), O.spectrum(X, Bv, dt, obs, e, bm.b.q, bm.b.current))
+    # flux and power density at random points
+    P = np.column_stack([rng.uniform(-5e-3, 5e-3, 29), rng.uniform(-5e-3, 5e-3, 29), rng.uniform(15, 35, 29)])
+    Nn = np.tile([0.0, 0.0, 1.0], (29, 1))
+    dp, dn, out = _dev(P.reshape(-1)), _dev(Nn.reshape(-1)), torch.empty(29, dtype=torch.float64, device="cuda")
+    _lib.check(L.srs_flux(view, beam, _vp(dp), 29, None, 411.0, _lib.FP64, _vp(out), None))
+    assert_fp64(out.cpu().numpy(), O.flux(X, Bv, dt, P, 411.0, bm.b.q, bm.b.current))
+    for directional in (0, 1):
+        _lib.check(L.srs_power_density(view, beam, _vp(dp), _vp(dn), 29, None, directional, _lib.FP64, _vp(out),
+                                       None))
+        assert_fp64(out.cpu().numpy(), O.power_density(X, Bv, A, dt, P, Nn, directional, bm.b.q, bm.b.current))
+
+
+def test_c_abi_rejects_bad_arguments():
+    from srsoriginal_b200 import _lib
+    view = _lib.TrajView(None, None, None, 0, 1, 1e-12)
+    with pytest.raises(ValueError):
+        _lib.check(_lib.lib.srs_spectrum(view, _lib.BeamConsts(-1.6e-19, 0.5), _lib.v3([0, 0, 1]), None, 0,
+                                         _lib.FP64, None, None))
+    with pytest.raises(ValueError, match="grid"):
+        t = _dev(np.zeros(30))
+        v = _lib.TrajView(C.cast(t.data_ptr(), _lib._D), C.cast(t.data_ptr(), _lib._D),
+                          C.cast(t.data_ptr(), _lib._D), 10, 1, 1e-12)
+        _lib.check(_lib.lib.srs_flux(v, _lib.BeamConsts(-1.6e-19, 0.5), _vp(t), 3, None, 100.0, _lib.MIXED,
+                                     _vp(t), None))
+
+
+def test_edge_cases_small_sizes():
+    o = new_sr(2)  # two trajectory points
+    s = o.calculate_spectrum(obs=[0, 0, 30], npoints=1, energy_range_eV=[150, 150])
+    assert len(s) == 1 and np.isfinite(s[0][1])
+    o = new_sr(201)
+    m = o.calculate_flux_rectangle(plane="XY", energy_eV=150.0, width=[0.01, 0.01], npoints=[1, 1],
+                                   translation=[0, 0, 30], precision="mixed")
+    assert len(m) == 1 and np.isfinite(m[0][1])
+    m = o.calculate_flux_rectangle(plane="XY", energy_eV=150.0, width=[0.01, 0.01], npoints=[1, 1],
+                                   translation=[0, 0, 30])
+    assert len(m) == 1
+
+
+# ------------------------------------------------------------------ mixed precision vs the reference
+
+def test_flux_cfg1_mixed_within_tolerance():
+    g = golden("flux_cfg1.npz")
+    o = new_sr(20001)
+    for tag in ("e1", "e3"):
+        pts, v = o.flux_arrays(float(g["energy_" + tag]), [101, 101], "XY", [0.01, 0.01], translation=[0, 0, 30],
+                               precision="mixed")
+        assert_mixed(v, g["flux_" + tag])
+
+
+def test_power_density_cfg2_mixed_within_tolerance():
+    g = golden("pd_cfg2.npz")
+    o = new_sr(40001, "epu")
+    pts, v = o.power_density_arrays([201, 201], "XY", [0.04, 0.04], translation=[0, 0, 30], precision="mixed")
+    assert_mixed(v, g["pd"])
+
+
+def test_spectrum_mixed_within_tolerance():
+    g = golden("spectrum_cfg0.npz")
+    o = new_sr(20001)
+    e, f = o.spectrum_arrays([0, 0, 30], 1000, [100, 1000], precision="mixed")
+    assert_mixed(f, g["flux"])
+    # non-uniform grid: one sincos per term
+    gm = golden("misc_fields.npz")
+    e, f = o.spectrum_arrays([0, 0, 30], points_eV=[151.0, 152.25225225225225, 455.0, 460.1], precision="mixed")
+    e2, f2 = o.spectrum_arrays([0, 0, 30], points_eV=[151.0, 152.25225225225225, 455.0, 460.1])
+    assert_mixed(f, f2)
