@@ -1,11 +1,24 @@
-// Fixed-step RK4 electron trajectories, one CUDA thread per particle (compiled with -fmad=false so
-// every operation rounds like the reference's x86-64 build).
+// Fixed-step RK4 electron trajectories (compiled with -fmad=false so every operation rounds like the
+// reference's x86-64 build).
 //
 // Reference: OSCARSSR::CalculateTrajectory (src/OSCARSSR.cc:562-673), DerivativesB (:741-765),
 // RK4 (:826-874).  State (x, vx, y, vy, z, vz) in m and m/s; dv/dt = (q/(m gamma)) v x B with gamma
 // fixed.  Forward from t0 for nforward points, then backward for nbackward points; the stored a/c at
 // a point is the derivative evaluated at the state of the previous step (the first forward point
 // stores 0, which the reference reads from an uninitialised array).
+//
+// The trajectory is a serial chain, so its cost is latency.  Two things shorten the chain without
+// changing a single rounding:
+//  * Field constants that the reference recomputes on every call (period length and direction,
+//    phase shift, region bounds, rotation sines/cosines) are computed once per launch, by the same
+//    IEEE operations, into shared memory.
+//  * Of the four field evaluations of an RK4 step, B(p0) and B(p0 + h/2 v0) need nothing but the
+//    step's start state, and once B(p0) is known so does B(p3) while B(p4) needs only B(p0) and
+//    B(p0 + h/2 v0): the step is two rounds of two independent evaluations.  In the warp-cooperative
+//    kernel one warp owns one particle and lanes (position slot, field) evaluate them side by side;
+//    warp shuffles gather the field sums in field order.  Every lane then advances the (identical)
+//    state redundantly, and nine lanes store the nine trajectory components of a point.
+// For very large batches one thread per particle (the plain kernel) gives better issue efficiency.
 //
 // Layout written: [particle][component][point], point index = time order (the backward points come
 // first, earliest at index 0), so no reversal pass is needed.
@@ -20,78 +33,257 @@ namespace {
 
 constexpr int kMaxFieldsShared = 16;
 
-__device__ inline void derivs(const srs_field *fields, int nf, const double x[6], double d[6], double qomg) {
-  V3 B = field_sum(fields, nf, v3(x[0], x[2], x[4]));
-  d[0] = x[1];
-  d[1] = qomg * (-x[5] * B.y + x[3] * B.z);
-  d[2] = x[3];
-  d[3] = qomg * (x[5] * B.x - x[1] * B.z);
-  d[4] = x[5];
-  d[5] = qomg * (x[1] * B.y - x[3] * B.x);
-}
+// Field constants the reference derives inside GetF (or in Init) from the descriptor.
+struct Prepared {
+  int kind;
+  double F[3], C[3], u[3];
+  double plen, ps, taper, b_lo, b_hi, e1_lo, e1_hi, e2_lo, e2_hi;  // undulator
+  double rs[3], rc[3];                                              // rotation sines / cosines
+};
 
-__device__ inline void rk4_step(const srs_field *fields, int nf, double y[6], const double dydx[6], double h,
-                                double qomg) {
-  double dym[6], dyt[6], yt[6];
-  const double hh = h * 0.5, h6 = h / 6.0;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) yt[i] = y[i] + hh * dydx[i];
-  derivs(fields, nf, yt, dyt, qomg);
-#pragma unroll
-  for (int i = 0; i < 6; ++i) yt[i] = y[i] + hh * dyt[i];
-  derivs(fields, nf, yt, dym, qomg);
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    yt[i] = y[i] + h * dym[i];
-    dym[i] += dyt[i];
+__device__ void prepare(const srs_field &f, Prepared &p) {
+  p.kind = f.kind;
+  for (int c = 0; c < 3; ++c) {
+    p.F[c] = f.field[c];
+    p.C[c] = f.center[c];
+    p.rs[c] = sin(f.rotations[c]);
+    p.rc[c] = cos(f.rotations[c]);
   }
-  derivs(fields, nf, yt, dyt, qomg);
-#pragma unroll
-  for (int i = 0; i < 6; ++i) y[i] = y[i] + h6 * (dydx[i] + dyt[i] + 2.0 * dym[i]);
+  if (f.kind == SRS_FIELD_UNDULATOR) {
+    // TField3D_IdealUndulator::Init (:62-80) and the per-call expressions of GetF (:106-139)
+    const V3 per = ld3(f.period);
+    p.plen = mag(per);
+    const V3 u = unit(per);
+    p.u[0] = u.x; p.u[1] = u.y; p.u[2] = u.z;
+    const double L = mag(per) * (f.nperiods + 2);
+    p.ps = f.phase * mag(per) / two_pi();
+    p.taper = f.taper;
+    p.b_hi = L / 2. + p.ps;
+    p.b_lo = -L / 2. + p.ps;
+    p.e1_lo = -L / 2. + p.ps + p.plen;
+    p.e1_hi = L / 2. + p.ps - p.plen;
+    p.e2_lo = -L / 2. + p.ps + p.plen / 2.;
+    p.e2_hi = L / 2. + p.ps - p.plen / 2.;
+  }
 }
 
-__global__ void rk4_kernel(const srs_field *__restrict__ gfields, int nfields,
-                           const srs_particle *__restrict__ particles, int nparticles, double dt,
-                           int64_t nfwd, int64_t nbwd, double *__restrict__ X, double *__restrict__ Bt,
-                           double *__restrict__ A) {
+// RotateSelfXYZ with the angles' sines and cosines precomputed (TVector3D.cc:150-205)
+__device__ inline V3 rotate_pre(V3 v, const Prepared &p) {
+  double t = v.y;
+  v.y = p.rc[0] * t - p.rs[0] * v.z;
+  v.z = p.rs[0] * t + p.rc[0] * v.z;
+  t = v.z;
+  v.z = p.rc[1] * t - p.rs[1] * v.x;
+  v.x = p.rs[1] * t + p.rc[1] * v.x;
+  t = v.x;
+  v.x = p.rc[2] * t - p.rs[2] * v.y;
+  v.y = p.rs[2] * t + p.rc[2] * v.y;
+  return v;
+}
+
+__device__ inline V3 field_one(const Prepared &p, const srs_field &f, V3 X) {
+  switch (p.kind) {
+    case SRS_FIELD_UNDULATOR: {
+      const double D = (X.x - p.C[0]) * p.u[0] + (X.y - p.C[1]) * p.u[1] + (X.z - p.C[2]) * p.u[2];
+      const double taper = 1 + D * p.taper;
+      if (D > p.b_hi || D < p.b_lo) return v3(0, 0, 0);
+      const double s = sin(two_pi() * (D - p.ps) / p.plen);
+      // ends: 0.25 / 0.75 of the field; the centre multiplies by 1.0, which is exact
+      const double fac = (D < p.e1_lo || D > p.e1_hi) ? ((D < p.e2_lo || D > p.e2_hi) ? 0.25 : 0.75) : 1.0;
+      return v3(p.F[0] * fac * s * taper, p.F[1] * fac * s * taper, p.F[2] * fac * s * taper);
+    }
+    case SRS_FIELD_GAUSSIAN: {
+      const V3 rx = rotate_pre(X, p) - ld3(p.C);
+      double frac = 1;
+      if (f.sigma_or_width[0] > 0) { double t = rx.x / f.sigma_or_width[0]; frac *= exp(-(t * t) / 2.); }
+      if (f.sigma_or_width[1] > 0) { double t = rx.y / f.sigma_or_width[1]; frac *= exp(-(t * t) / 2.); }
+      if (f.sigma_or_width[2] > 0) { double t = rx.z / f.sigma_or_width[2]; frac *= exp(-(t * t) / 2.); }
+      return ld3(p.F) * frac;
+    }
+    case SRS_FIELD_UNIFORM_BOX: {
+      const V3 rx = rotate_pre(X, p) - ld3(p.C);
+      const double *w = f.sigma_or_width;
+      if ((!(w[0] <= 0) && fabs(rx.x) > fabs(w[0] / 2.)) || (!(w[1] <= 0) && fabs(rx.y) > fabs(w[1] / 2.)) ||
+          (!(w[2] <= 0) && fabs(rx.z) > fabs(w[2] / 2.)))
+        return v3(0, 0, 0);
+      return ld3(p.F);
+    }
+    case SRS_FIELD_GRID:
+      return grid_field(f, X);
+    default:
+      return v3(0, 0, 0);
+  }
+}
+
+// DerivativesB (OSCARSSR.cc:741-765): the velocity part
+__device__ inline V3 force(double qomg, V3 v, V3 B) {
+  return v3(qomg * (-v.z * B.y + v.y * B.z), qomg * (v.z * B.x - v.x * B.z), qomg * (v.x * B.y - v.y * B.x));
+}
+
+__device__ inline V3 vadd_scaled(V3 a, double h, V3 b) { return v3(a.x + h * b.x, a.y + h * b.y, a.z + h * b.z); }
+
+// ---------------------------------------------------------------- warp-cooperative kernel
+
+__global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restrict__ gfields, int nfields,
+                                                       const srs_particle *__restrict__ particles, int nparticles,
+                                                       double dt, int64_t nfwd, int64_t nbwd,
+                                                       double *__restrict__ X, double *__restrict__ Bt,
+                                                       double *__restrict__ A) {
   __shared__ srs_field sf[kMaxFieldsShared];
-  const srs_field *fields = gfields;
-  if (nfields <= kMaxFieldsShared) {
-    for (int i = threadIdx.x; i < nfields; i += blockDim.x) sf[i] = gfields[i];
-    __syncthreads();
-    fields = sf;
+  __shared__ Prepared sp[kMaxFieldsShared];
+  for (int i = threadIdx.x; i < nfields; i += blockDim.x) {
+    sf[i] = gfields[i];
+    prepare(sf[i], sp[i]);
   }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (p >= nparticles) return;  // whole warps exit together
+  const srs_particle P = particles[p];
+  const int64_t n = nfwd + nbwd;
+  double *out = nullptr;  // this lane's output component (lanes 0..8)
+  if (lane < 3) out = X + (int64_t)p * 3 * n + lane * n;
+  else if (lane < 6) out = Bt + (int64_t)p * 3 * n + (lane - 3) * n;
+  else if (lane < 9) out = A + (int64_t)p * 3 * n + (lane - 6) * n;
+  const int slot = nfields > 0 ? lane / nfields : 2, fidx = nfields > 0 ? lane % nfields : 0;
+  const bool evaluates = slot < 2;
+  const double C = kC, qomg = P.qomg;
+  const unsigned full = 0xffffffffu;
+
+  // B at two positions, one per slot, summed over fields in field order
+  auto fields2 = [&](V3 pa, V3 pb, V3 &Ba, V3 &Bb) {
+    V3 mine = v3(0, 0, 0);
+    if (evaluates) mine = field_one(sp[fidx], sf[fidx], slot == 0 ? pa : pb);
+    Ba = v3(0, 0, 0);
+    Bb = v3(0, 0, 0);
+    for (int f = 0; f < nfields; ++f) {
+      Ba = Ba + v3(__shfl_sync(full, mine.x, f), __shfl_sync(full, mine.y, f), __shfl_sync(full, mine.z, f));
+      Bb = Bb + v3(__shfl_sync(full, mine.x, nfields + f), __shfl_sync(full, mine.y, nfields + f),
+                   __shfl_sync(full, mine.z, nfields + f));
+    }
+  };
+  auto store = [&](int64_t k, V3 pos, V3 vel, V3 acc) {
+    double v = 0;
+    switch (lane) {
+      case 0: v = pos.x; break;
+      case 1: v = pos.y; break;
+      case 2: v = pos.z; break;
+      case 3: v = vel.x / C; break;
+      case 4: v = vel.y / C; break;
+      case 5: v = vel.z / C; break;
+      case 6: v = acc.x / C; break;
+      case 7: v = acc.y / C; break;
+      case 8: v = acc.z / C; break;
+    }
+    if (out) out[k] = v;
+  };
+  // one RK4 step of size h from (pos, vel); returns the derivative at the start state (its velocity part)
+  auto step = [&](V3 &pos, V3 &vel, double h) -> V3 {
+    const double hh = h * 0.5, h6 = h / 6.0;
+    V3 B1, B2, B3, B4;
+    const V3 p2 = vadd_scaled(pos, hh, vel);          // yt = y + hh*dydx (positions)
+    fields2(pos, p2, B1, B2);
+    const V3 a1 = force(qomg, vel, B1);                // dydx (velocity part)
+    const V3 v2 = vadd_scaled(vel, hh, a1);
+    const V3 a2 = force(qomg, v2, B2);                 // dyt
+    const V3 p3 = vadd_scaled(pos, hh, v2);            // yt = y + hh*dyt
+    const V3 v3_ = vadd_scaled(vel, hh, a2);
+    const V3 p4 = vadd_scaled(pos, h, v3_);            // yt = y + h*dym (positions need dym = dyt(p3) pos part = v3)
+    // dym = f(yt3): position part v3_, velocity part a3 = force(v3_, B(p3))
+    fields2(p3, p4, B3, B4);
+    const V3 a3 = force(qomg, v3_, B3);
+    const V3 v4 = vadd_scaled(vel, h, a3);             // yt = y + h*dym (velocities)
+    const V3 m_pos = v3_ + v2, m_vel = a3 + a2;        // dym += dyt
+    const V3 a4 = force(qomg, v4, B4);                 // dyt = f(yt4): position part v4
+    // yout = y + h6*(dydx + dyt + 2.0*dym)
+    const V3 npos = v3(pos.x + h6 * (vel.x + v4.x + 2.0 * m_pos.x), pos.y + h6 * (vel.y + v4.y + 2.0 * m_pos.y),
+                       pos.z + h6 * (vel.z + v4.z + 2.0 * m_pos.z));
+    const V3 nvel = v3(vel.x + h6 * (a1.x + a4.x + 2.0 * m_vel.x), vel.y + h6 * (a1.y + a4.y + 2.0 * m_vel.y),
+                       vel.z + h6 * (a1.z + a4.z + 2.0 * m_vel.z));
+    pos = npos;
+    vel = nvel;
+    return a1;
+  };
+
+  const V3 pos0 = v3(P.x0[0], P.x0[1], P.x0[2]);
+  const V3 vel0 = v3(P.beta0[0] * C, P.beta0[1] * C, P.beta0[2] * C);
+  V3 pos = pos0, vel = vel0, acc = v3(0, 0, 0);
+  for (int64_t i = 0; i < nfwd; ++i) {
+    store(nbwd + i, pos, vel, acc);
+    acc = step(pos, vel, dt);
+  }
+  pos = pos0;
+  vel = vel0;
+  const double mdt = -dt;
+  for (int64_t i = 0; i < nbwd; ++i) {
+    acc = step(pos, vel, mdt);
+    store(nbwd - 1 - i, pos, vel, acc);
+  }
+}
+
+// ---------------------------------------------------------------- one thread per particle
+
+__global__ void __launch_bounds__(64) rk4_thread_kernel(const srs_field *__restrict__ gfields, int nfields,
+                                                        const srs_particle *__restrict__ particles, int nparticles,
+                                                        double dt, int64_t nfwd, int64_t nbwd,
+                                                        double *__restrict__ X, double *__restrict__ Bt,
+                                                        double *__restrict__ A) {
+  __shared__ srs_field sf[kMaxFieldsShared];
+  __shared__ Prepared sp[kMaxFieldsShared];
+  for (int i = threadIdx.x; i < nfields; i += blockDim.x) {
+    sf[i] = gfields[i];
+    prepare(sf[i], sp[i]);
+  }
+  __syncthreads();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nparticles) return;
   const srs_particle P = particles[p];
   const int64_t n = nfwd + nbwd;
   double *xp = X + (int64_t)p * 3 * n, *bp = Bt + (int64_t)p * 3 * n, *ap = A + (int64_t)p * 3 * n;
-  const double C = kC;
-  double x[6] = {P.x0[0], P.beta0[0] * C, P.x0[1], P.beta0[1] * C, P.x0[2], P.beta0[2] * C};
-  double d[6] = {0, 0, 0, 0, 0, 0};
-  auto store = [&](int64_t k) {
-    xp[k] = x[0];
-    xp[n + k] = x[2];
-    xp[2 * n + k] = x[4];
-    bp[k] = x[1] / C;
-    bp[n + k] = x[3] / C;
-    bp[2 * n + k] = x[5] / C;
-    ap[k] = d[1] / C;
-    ap[n + k] = d[3] / C;
-    ap[2 * n + k] = d[5] / C;
+  const double C = kC, qomg = P.qomg;
+  auto Bsum = [&](V3 x) {
+    V3 s = v3(0, 0, 0);
+    for (int f = 0; f < nfields; ++f) s = s + field_one(sp[f], sf[f], x);
+    return s;
   };
-  x[0] = P.x0[0]; x[1] = P.beta0[0] * C; x[2] = P.x0[1]; x[3] = P.beta0[1] * C; x[4] = P.x0[2]; x[5] = P.beta0[2] * C;
+  auto step = [&](V3 &pos, V3 &vel, double h) -> V3 {
+    const double hh = h * 0.5, h6 = h / 6.0;
+    const V3 p2 = vadd_scaled(pos, hh, vel);
+    const V3 a1 = force(qomg, vel, Bsum(pos));
+    const V3 v2 = vadd_scaled(vel, hh, a1);
+    const V3 a2 = force(qomg, v2, Bsum(p2));
+    const V3 p3 = vadd_scaled(pos, hh, v2);
+    const V3 v3_ = vadd_scaled(vel, hh, a2);
+    const V3 a3 = force(qomg, v3_, Bsum(p3));
+    const V3 p4 = vadd_scaled(pos, h, v3_);
+    const V3 v4 = vadd_scaled(vel, h, a3);
+    const V3 m_pos = v3_ + v2, m_vel = a3 + a2;
+    const V3 a4 = force(qomg, v4, Bsum(p4));
+    const V3 npos = v3(pos.x + h6 * (vel.x + v4.x + 2.0 * m_pos.x), pos.y + h6 * (vel.y + v4.y + 2.0 * m_pos.y),
+                       pos.z + h6 * (vel.z + v4.z + 2.0 * m_pos.z));
+    const V3 nvel = v3(vel.x + h6 * (a1.x + a4.x + 2.0 * m_vel.x), vel.y + h6 * (a1.y + a4.y + 2.0 * m_vel.y),
+                       vel.z + h6 * (a1.z + a4.z + 2.0 * m_vel.z));
+    pos = npos;
+    vel = nvel;
+    return a1;
+  };
+  auto store = [&](int64_t k, V3 pos, V3 vel, V3 acc) {
+    xp[k] = pos.x; xp[n + k] = pos.y; xp[2 * n + k] = pos.z;
+    bp[k] = vel.x / C; bp[n + k] = vel.y / C; bp[2 * n + k] = vel.z / C;
+    ap[k] = acc.x / C; ap[n + k] = acc.y / C; ap[2 * n + k] = acc.z / C;
+  };
+  const V3 pos0 = v3(P.x0[0], P.x0[1], P.x0[2]);
+  const V3 vel0 = v3(P.beta0[0] * C, P.beta0[1] * C, P.beta0[2] * C);
+  V3 pos = pos0, vel = vel0, acc = v3(0, 0, 0);
   for (int64_t i = 0; i < nfwd; ++i) {
-    store(nbwd + i);
-    derivs(fields, nfields, x, d, P.qomg);
-    rk4_step(fields, nfields, x, d, dt, P.qomg);
+    store(nbwd + i, pos, vel, acc);
+    acc = step(pos, vel, dt);
   }
-  x[0] = P.x0[0]; x[1] = P.beta0[0] * C; x[2] = P.x0[1]; x[3] = P.beta0[1] * C; x[4] = P.x0[2]; x[5] = P.beta0[2] * C;
-  const double mdt = -dt;
+  pos = pos0;
+  vel = vel0;
   for (int64_t i = 0; i < nbwd; ++i) {
-    derivs(fields, nfields, x, d, P.qomg);
-    rk4_step(fields, nfields, x, d, mdt, P.qomg);
-    store(nbwd - 1 - i);
+    acc = step(pos, vel, -dt);
+    store(nbwd - 1 - i, pos, vel, acc);
   }
 }
 
@@ -111,10 +303,17 @@ cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particl
                        double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
                        cudaStream_t s) {
   if (nparticles <= 0) return cudaSuccess;
-  // Small blocks: a latency-bound serial loop per thread; spread particles over all SMs.
-  const int threads = nparticles >= 148 * 64 ? 64 : 32;
-  const int blocks = (nparticles + threads - 1) / threads;
-  rk4_kernel<<<blocks, threads, 0, s>>>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a);
+  if (nfields > kMaxFieldsShared) return cudaErrorInvalidValue;
+  if (2 * nfields <= 32 && nparticles <= 16384) {
+    const int warps = 4;
+    rk4_warp_kernel<<<(nparticles + warps - 1) / warps, 32 * warps, 0, s>>>(d_fields, nfields, d_particles,
+                                                                            nparticles, dt, nfwd, nbwd, d_x, d_b, d_a);
+  } else {
+    const int threads = 64;
+    rk4_thread_kernel<<<(nparticles + threads - 1) / threads, threads, 0, s>>>(d_fields, nfields, d_particles,
+                                                                               nparticles, dt, nfwd, nbwd, d_x, d_b,
+                                                                               d_a);
+  }
   return cudaGetLastError();
 }
 

@@ -175,7 +175,10 @@ __global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__rest
                                                             const double *__restrict__ Ac, int64_t n, srs_grid2d g,
                                                             double nx_, double ny_, double nz_, int directional,
                                                             int64_t chunk, double *__restrict__ partial) {
-  __shared__ float sm[17][kSub];
+  // (1 - n.beta)^5 ~ 1e-39 does not fit FP32, so the FP32 term is scaled: with omb = 1 - |beta|,
+  // 1 - n.beta = omb_i * opn, opn = 1 + (|beta|/(2 omb_i)) |n - bhat|^2 >= 1, and
+  // 1/(1 - n.beta)^5 = (omb_ref/omb_i)^5 / opn^5 / omb_ref^5; the last factor (~1e39) is applied in FP64.
+  __shared__ float sm[18][kSub];
   const int tid = threadIdx.x;
   const int nt2 = (g.n2 + kTileB - 1) / kTileB;
   const int T1 = blockIdx.x / nt2, T2 = blockIdx.x % nt2;
@@ -196,6 +199,12 @@ __global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__rest
   for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);
   const float dd = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
   const float nrx = (float)nx_, nry = (float)ny_, nrz = (float)nz_;
+  double omb_ref;
+  {
+    const double bx = bp[0], by = bp[n], bz = bp[2 * n];
+    const double b2 = bx * bx + by * by + bz * bz;
+    omb_ref = (1.0 - b2) / (1.0 + sqrt(b2));
+  }
   double sum = 0;
   for (int64_t base = i0; base < iend; base += kSub) {
     const int cnt = (int)imin64(kSub, iend - base);
@@ -204,10 +213,11 @@ __global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__rest
       const int64_t i = base + tid;
       const Anchor A = make_anchor(Oc, xp, bp, n, i);
       const double ax = ap[i], ay = ap[n + i], az = ap[2 * n + i];
+      const double r = omb_ref / A.omb;
       sm[0][tid] = (float)A.invDc;
       sm[1][tid] = (float)A.Dc;
       sm[2][tid] = (float)A.omb;
-      sm[3][tid] = (float)(0.5 * A.bmag);
+      sm[3][tid] = (float)(0.5 * A.bmag / A.omb);
       sm[4][tid] = (float)(A.bhat[0] * ax + A.bhat[1] * ay + A.bhat[2] * az);  // bhat . a
       for (int c = 0; c < 3; ++c) {
         sm[5 + c][tid] = (float)A.nc[c];
@@ -215,6 +225,7 @@ __global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__rest
         sm[11 + c][tid] = (float)(A.bhat[c] * A.omb);
       }
       sm[14][tid] = (float)ax; sm[15][tid] = (float)ay; sm[16][tid] = (float)az;
+      sm[17][tid] = (float)(r * r * r * r * r);
     }
     __syncthreads();
     if (!active) continue;
@@ -233,20 +244,22 @@ __global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__rest
       const float nd = fmaf(nz, nrz, fmaf(ny, nry, nx * nrx));
       if (directional && nd <= 0.0f) continue;
       const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-      const float opnb = fmaf(sm[3][k], d2, sm[2][k]);  // 1 - n.beta
+      const float opn = fmaf(sm[3][k], d2, 1.0f);  // (1 - n.beta) / omb_i
+      const float opnb = sm[2][k] * opn;           // 1 - n.beta
       const float axx = sm[14][k], ayy = sm[15][k], azz = sm[16][k];
       const float na = fmaf(dz, azz, fmaf(dy, ayy, fmaf(dx, axx, sm[4][k])));  // n . a
       // V = n x ((n - beta) x a) = (n - beta)(n.a) - a (1 - n.beta)
       const float Xx = dx + sm[11][k], Xy = dy + sm[12][k], Xz = dz + sm[13][k];
       const float Vx = fmaf(Xx, na, -axx * opnb), Vy = fmaf(Xy, na, -ayy * opnb), Vz = fmaf(Xz, na, -azz * opnb);
       const float v2 = fmaf(Vz, Vz, fmaf(Vy, Vy, Vx * Vx));
-      const float o2 = opnb * opnb;
-      const float o5 = o2 * o2 * opnb;
-      acc = fmaf(v2 * rinv * rinv * nd, __fdividef(1.0f, o5), acc);
+      const float o2 = opn * opn;
+      const float o5 = o2 * o2 * opn;
+      acc = fmaf(v2 * rinv * rinv * nd * sm[17][k], __fdividef(1.0f, o5), acc);
     }
     sum += (double)acc;
   }
-  if (active) partial[((int64_t)p * S + s) * np + j] = sum;
+  const double r2 = 1.0 / (omb_ref * omb_ref);
+  if (active) partial[((int64_t)p * S + s) * np + j] = sum * (r2 * r2 / omb_ref);
 }
 
 // ---------------------------------------------------------------- spectrum at one observer

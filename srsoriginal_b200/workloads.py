@@ -81,11 +81,11 @@ def write_oscars_grid(path, z, by, bx=None):
     (header: comment, then start/step/count for x, y and z; then 'Bx By Bz' per sample)."""
     z = np.asarray(z, dtype=np.float64)
     bx = np.zeros_like(by) if bx is None else bx
-    dz = (z[-1] - z[0]) / (len(z) - 1)
+    dz = float((z[-1] - z[0]) / (len(z) - 1))
     with open(path, "w") as f:
         f.write("# OSCARS 1-D field map\n")
         f.write("0\n0\n1\n0\n0\n1\n")
-        f.write(f"{z[0]!r}\n{dz!r}\n{len(z)}\n")
+        f.write(f"{float(z[0])!r}\n{dz!r}\n{len(z)}\n")
         for i in range(len(z)):
             f.write(f"{float(bx[i])!r} {float(by[i])!r} 0.0\n")
 

@@ -200,13 +200,14 @@ def quirks():
 
 
 if __name__ == "__main__":
-    e1 = cfg0()
-    print("E1 (first-harmonic peak of the config-0 spectrum):", repr(e1))
-    if abs(e1 - W.E1_EV) > 1e-9:
-        print("NOTE: update workloads.E1_EV to", repr(e1))
-    cfg1(e1)
-    cfg2()
-    misc()
-    beam()
-    grid()
-    quirks()
+    parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "grid", "quirks"]
+    if "cfg0" in parts:
+        e1 = cfg0()
+        print("E1 (first-harmonic peak of the config-0 spectrum):", repr(e1))
+        if abs(e1 - W.E1_EV) > 1e-9:
+            print("NOTE: update workloads.E1_EV to", repr(e1))
+    if "cfg1" in parts:
+        cfg1(W.E1_EV)
+    for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("grid", grid), ("quirks", quirks)):
+        if name in parts:
+            fn()
