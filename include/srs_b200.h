@@ -152,6 +152,22 @@ srs_status srs_flux(srs_traj_view traj, srs_beam_consts beam, const double *d_po
                     const srs_grid2d *grid, double energy_ev, int32_t precision, double *d_out,
                     void *stream);
 
+/* srs_flux with SRS_PRECISION_MIXED on a grid, allocating nothing.  No counterpart in the
+ * reference.  For callers that must not allocate device memory while they run (their device memory
+ * is reserved up front by their own allocator, or a loop that may not call cudaMalloc, whose latency
+ * is unbounded and which can synchronise the device).  srs_flux takes its scratch (per-chunk partial
+ * sums) from a stream-ordered allocation; this entry point uses a fixed 8 MiB array that the library
+ * defines in device memory instead, which every GPU that loads the library holds until the process
+ * exits.  Limit: nparticles * grid->n1 * grid->n2 <= 174762 (SRS_ERR_RANGE beyond that, with a
+ * message).  The caller still passes the trajectory and the output (DEVICE memory).  All calls share
+ * the array and it keeps the last call's contents, so calls that overlap on the GPU (other streams,
+ * other host threads) race: serialise them.  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that first call before any
+ * stream capture.  Results equal srs_flux's to rounding (the partial sums may be split into fewer
+ * trajectory chunks). */
+srs_status srs_flux_mixed_noalloc(srs_traj_view traj, srs_beam_consts beam, const srs_grid2d *grid,
+                                  double energy_ev, double *d_out, void *stream);
+
 /* Power density at np points with unit normals (OSCARSSR.cc:1477-1598; the reference's CPU
  * semantics: with directional != 0 the terms with n.normal <= 0 are skipped, otherwise the result is
  * made non-negative).  d_points, d_normals: DEVICE 3*np doubles.  d_out: DEVICE nparticles*np values

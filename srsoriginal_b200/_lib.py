@@ -112,6 +112,7 @@ def _load():
                                                 C.c_int32, C.c_int32, C.c_int32, _D, _D]),
         "srs_sim_calculate_total_power": (S, [P, _D]),
         "srs_measure_peak": (S, [C.c_int32, _D, P]),
+        "srs_flux_mixed_noalloc": (S, [TrajView, BeamConsts, C.POINTER(Grid2D), C.c_double, P, P]),
         "srs_energy_grid": (S, [C.c_int64, C.c_double, C.c_double, _D]),
         "srs_rectangle_plane": (S, [C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_double, _D, _D,
                                     C.c_int32, _D, _D, _D, C.POINTER(Grid2D)]),
@@ -138,7 +139,7 @@ EXPORTED = (
     "srs_sim_get_particle srs_set_seed srs_random_uniform srs_random_normal srs_random_reset "
     "srs_sim_calculate_trajectory srs_sim_calculate_spectrum srs_sim_calculate_flux "
     "srs_sim_calculate_power_density srs_sim_calculate_total_power srs_energy_grid "
-    "srs_rectangle_plane srs_rectangle_points srs_measure_peak"
+    "srs_rectangle_plane srs_rectangle_points srs_measure_peak srs_flux_mixed_noalloc"
 ).split()
 
 

@@ -27,6 +27,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "srs_device.cuh"
@@ -389,9 +391,8 @@ size_t mixed_flux_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles) 
   return sizeof(double) * 6 * (size_t)g.n1 * g.n2 * nparticles * flux_mixed_splits(n, g, nparticles);
 }
 
-cudaError_t mixed_flux(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g, double energy_ev,
-                       double *d_out, void *scratch, cudaStream_t s) {
-  const int S = flux_mixed_splits(t.n, g, t.nparticles);
+static cudaError_t mixed_flux_splits(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g,
+                                     double energy_ev, double *d_out, void *scratch, int S, cudaStream_t s) {
   const int64_t chunk = (t.n + S - 1) / S;
   GridTiles tl = tiles_of(g);
   const double omega = ev_to_omega(energy_ev);
@@ -403,6 +404,76 @@ cudaError_t mixed_flux(const srs_traj_view &t, const srs_beam_consts &b, const s
   return finish_flux_partials(partial, S, (int64_t)g.n1 * g.n2, t.nparticles, nullptr, omega, t.dt, flux_c0(b.charge),
                               flux_c2(b.charge, b.current), d_out, s);
 }
+
+cudaError_t mixed_flux(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g, double energy_ev,
+                       double *d_out, void *scratch, cudaStream_t s) {
+  return mixed_flux_splits(t, b, g, energy_ev, d_out, scratch, flux_mixed_splits(t.n, g, t.nparticles), s);
+}
+
+// ---------------------------------------------------------------- allocation-free flux entry point
+//
+// For callers that must not allocate device memory once they are running -- for example a host
+// program whose device memory is entirely reserved up front by its own allocator, or a
+// latency-critical loop that forbids cudaMalloc (which can synchronise the device and has no bounded
+// latency).  The per-chunk partial sums that srs_flux keeps in a stream-ordered allocation live
+// here in a fixed, file-scope device array instead.
+//
+// Every GPU that loads this library holds this array until the process exits.  All calls share it,
+// and it keeps the last call's contents: calls that overlap on the GPU (different streams, or
+// several host threads) race on it, so the caller must serialise them.  Nothing in it needs to start
+// at zero: each call's main kernel writes every slot that its finishing kernel reads.
+constexpr size_t kNoAllocScratchDoubles = (size_t)1 << 20;  // 8 MiB
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+// Device address of g_noalloc_scratch, looked up once per device.  In host code the array's name is
+// only a host-side stand-in, so the address must come from cudaGetSymbolAddress with the device
+// current.
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[64];
+
+static cudaError_t noalloc_scratch(void **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace srs
+
+extern "C" srs_status srs_flux_mixed_noalloc(srs_traj_view traj, srs_beam_consts beam, const srs_grid2d *grid,
+                                             double energy_ev, double *d_out, void *stream) {
+  using namespace srs;
+  clear_error();
+  if (!traj.x || !traj.beta || traj.n < 1 || traj.nparticles < 1 || !(traj.dt > 0))
+    return fail(SRS_ERR_INVALID, "bad trajectory view");
+  if (!grid || grid->n1 < 1 || grid->n2 < 1) return fail(SRS_ERR_INVALID, "the points must be given as a grid");
+  if (!d_out) return fail(SRS_ERR_INVALID, "NULL output");
+  if (!(energy_ev > 0)) return fail(SRS_ERR_INVALID, "energy_eV must be > 0");
+  // partial sums: 6 doubles per (particle, point, trajectory chunk); use as many chunks as fit
+  const size_t per_chunk = (size_t)6 * grid->n1 * grid->n2 * traj.nparticles;
+  if (per_chunk > kNoAllocScratchDoubles)
+    return fail(SRS_ERR_RANGE, "srs_flux_mixed_noalloc: nparticles * points = " +
+                                   std::to_string((size_t)grid->n1 * grid->n2 * traj.nparticles) +
+                                   " exceeds its fixed scratch (at most " +
+                                   std::to_string(kNoAllocScratchDoubles / 6) + " particle-points); use srs_flux");
+  const int S = (int)std::max<size_t>(1, std::min<size_t>((size_t)flux_mixed_splits(traj.n, *grid, traj.nparticles),
+                                                          kNoAllocScratchDoubles / per_chunk));
+  void *scratch = nullptr;
+  SRS_CUDA(noalloc_scratch(&scratch));
+  SRS_CUDA(mixed_flux_splits(traj, beam, *grid, energy_ev, d_out, scratch, S, static_cast<cudaStream_t>(stream)));
+  return SRS_OK;
+}
+
+namespace srs {
 
 size_t mixed_pd_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles) {
   GridTiles tl = tiles_of(g);
