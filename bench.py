@@ -37,12 +37,10 @@ EVALS_PER_STEP = len(ENERGIES) * NT * GRID_N * GRID_N
 METRIC = "integrand evals/s (mixed vs plain FP64 at <=1e-4 rel flux err)"
 UNIT = "evals/s"
 
-# Algorithmic work per integrand evaluation of the mixed flux kernel (per (trajectory point,
-# observation point) pair; FP32 instructions with an FMA counted as one, MUFU ops, FP64 instructions).
-# Per pair: D_j - D_c (g: 3, h: 1, second-order term: 3, total: 1), 1/D_j (1 + 1 MUFU), phase (3),
-# reduction mod 2pi (5), sincos (1 + 2 MUFU), n_j - n_c (6), amplitude (9), complex MAC (12).
-# The per-(trajectory point, tile) FP64 anchor (~60 FP64 instructions per 128 pairs) is < 0.5 per pair.
-OPS_PER_EVAL = {"fp32": 45.0, "sfu": 3.0, "fp64": 0.5}
+# Algorithmic work per integrand evaluation of a flux map (one trajectory point x one observation
+# point), frozen in srsoriginal_b200/roofline_counts.json before measurement: FP64 (R 3, |R|^2 5,
+# sqrt 1, tau 2, phase and its reduction 3), FP32 (n 4, amplitude 11, MACs 24), SFU (sincos 2).
+OPS_PER_EVAL = json.load(open(os.path.join(ROOT, "srsoriginal_b200", "roofline_counts.json")))["flux_map_mixed"]
 
 
 def log(*a):
@@ -93,18 +91,23 @@ class ClockSampler:
         self.path = None
 
     def start(self):
+        """Starts sampling every 100 ms and returns once the first sample is on disk."""
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                                          "--format=csv,noheader,nounits", "-lms", "100", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 10 and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)  # one more sample after the timed region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -290,30 +293,35 @@ def run_ours(args, world, rank, local):
     if os.path.exists(traffic_file):
         roofline["traffic"] = json.load(open(traffic_file)).get("bytes_per_launch")
 
-    # e2e through the public API (host buffers, synchronous calls)
+    # e2e through the public API (host buffers, synchronous calls).  One step = what a user does for
+    # config 1: the trajectory (RK4 on the GPU, once: the object drops its kept trajectory at the start
+    # of every step) and both maps, with the host<->device copies of each call.
     o = sr()
     W.setup_beam(o, NT)
     W.setup_undulator(o)
     e2e_steps = max(1, min(args.steps, 10))
-    for _ in range(min(2, args.warmup)):
+
+    def e2e_step():
+        o.set_trajectory_cache(True)  # drops the kept trajectory: this step integrates it again
         for e in ENERGIES:
             o.flux_arrays(e, [GRID_N, GRID_N], "XY", [WIDTH, WIDTH], translation=[0, 0, W.SCREEN_Z],
                           precision="mixed")
+
+    for _ in range(min(2, args.warmup)):
+        e2e_step()
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        for e in ENERGIES:
-            o.flux_arrays(e, [GRID_N, GRID_N], "XY", [WIDTH, WIDTH], translation=[0, 0, W.SCREEN_Z],
-                          precision="mixed")
+        e2e_step()
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e = {"value": world * EVALS_PER_STEP * e2e_steps / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": len(ENERGIES) * (npts * 3 * 8 + 2 * npts * 8 + 248 + 56),
+           # per map: accumulator and compensation arrays in, particle in (RK4 once per step); out: both arrays
+           "h2d_bytes_per_step": len(ENERGIES) * 2 * npts * 8 + 56,
            "d2h_bytes_per_step": len(ENERGIES) * 2 * npts * 8,
            "ms_per_step": 1e3 * e2e_s / e2e_steps,
-           "includes": "RK4 trajectory on the GPU per map, H2D of points/fields/particle/accumulators, both "
-                       "maps, D2H of results"}
+           "includes": "RK4 trajectory on the GPU (once per step), both maps, host<->device copies of each call"}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -343,7 +351,7 @@ def run_ours(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

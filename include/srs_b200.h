@@ -221,6 +221,11 @@ srs_status srs_sim_add_bfield_grid(srs_sim *sim, const double start[3], const do
                                    const int64_t n[3], const double *data, const double rotations[3],
                                    const double translation[3]);
 srs_status srs_sim_clear_bfields(srs_sim *sim);
+/* The object keeps the device trajectory of its last single-particle calculation and reuses it
+ * while the particle, the fields and the trajectory settings are unchanged (the reference recomputes
+ * the identical trajectory on every call).  enabled = 0 turns this off; every call drops the kept
+ * trajectory.  No counterpart in the reference. */
+srs_status srs_sim_set_trajectory_cache(srs_sim *sim, int32_t enabled);
 int32_t srs_sim_get_nfields(srs_sim *sim);
 /* Field at points (evaluated on the device): xyz and out are HOST arrays of 3*np doubles. */
 srs_status srs_sim_get_bfield(srs_sim *sim, const double *xyz, int64_t np, double *out);

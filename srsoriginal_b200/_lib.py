@@ -92,6 +92,7 @@ def _load():
         "srs_sim_add_bfield_file": (S, [P, C.c_char_p, C.c_char_p, _D, _D, _D, C.c_int32]),
         "srs_sim_add_bfield_grid": (S, [P, _D, _D, C.POINTER(C.c_int64), _D, _D, _D]),
         "srs_sim_clear_bfields": (S, [P]),
+        "srs_sim_set_trajectory_cache": (S, [P, C.c_int32]),
         "srs_sim_get_nfields": (C.c_int32, [P]),
         "srs_sim_get_bfield": (S, [P, _D, C.c_int64, _D]),
         "srs_sim_set_field_grid_data": (S, [P, C.c_int32, P, C.c_int32]),
@@ -134,6 +135,7 @@ EXPORTED = (
     "srs_sim_get_npoints_trajectory srs_sim_set_nthreads_global srs_sim_set_gpu_global "
     "srs_sim_add_bfield_undulator srs_sim_add_bfield_gaussian srs_sim_add_bfield_uniform "
     "srs_sim_add_bfield_file srs_sim_add_bfield_grid srs_sim_clear_bfields srs_sim_get_nfields "
+    "srs_sim_set_trajectory_cache "
     "srs_sim_get_bfield srs_sim_set_field_grid_data srs_sim_add_particle_beam "
     "srs_sim_clear_particle_beams srs_sim_get_nparticle_beams srs_sim_set_new_particle "
     "srs_sim_get_particle srs_set_seed srs_random_uniform srs_random_normal srs_random_reset "

@@ -33,12 +33,21 @@ namespace {
 
 constexpr int kMaxFieldsShared = 16;
 
+// a / b rounded to nearest, given rb = RN(1/b): one multiply and Markstein's FMA correction step
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990): with q = RN(a rb) faithful and r = a - b q exact,
+// RN(q + r rb) = RN(a / b) for normal operands without overflow or underflow.
+__device__ __forceinline__ double div_rn(double a, double b, double rb) {
+  const double q = __dmul_rn(a, rb);
+  const double r = __fma_rn(-q, b, a);
+  return __fma_rn(r, rb, q);
+}
+
 // Field constants the reference derives inside GetF (or in Init) from the descriptor.
 struct Prepared {
   int kind;
   double F[3], C[3], u[3];
-  double plen, ps, taper, b_lo, b_hi, e1_lo, e1_hi, e2_lo, e2_hi;  // undulator
-  double rs[3], rc[3];                                              // rotation sines / cosines
+  double plen, rplen, ps, taper, b_lo, b_hi, e1_lo, e1_hi, e2_lo, e2_hi;  // undulator
+  double rs[3], rc[3];                                                     // rotation sines / cosines
 };
 
 __device__ void prepare(const srs_field &f, Prepared &p) {
@@ -53,6 +62,7 @@ __device__ void prepare(const srs_field &f, Prepared &p) {
     // TField3D_IdealUndulator::Init (:62-80) and the per-call expressions of GetF (:106-139)
     const V3 per = ld3(f.period);
     p.plen = mag(per);
+    p.rplen = 1.0 / p.plen;
     const V3 u = unit(per);
     p.u[0] = u.x; p.u[1] = u.y; p.u[2] = u.z;
     const double L = mag(per) * (f.nperiods + 2);
@@ -87,7 +97,7 @@ __device__ inline V3 field_one(const Prepared &p, const srs_field &f, V3 X) {
       const double D = (X.x - p.C[0]) * p.u[0] + (X.y - p.C[1]) * p.u[1] + (X.z - p.C[2]) * p.u[2];
       const double taper = 1 + D * p.taper;
       if (D > p.b_hi || D < p.b_lo) return v3(0, 0, 0);
-      const double s = sin(two_pi() * (D - p.ps) / p.plen);
+      const double s = sin(div_rn(two_pi() * (D - p.ps), p.plen, p.rplen));
       // ends: 0.25 / 0.75 of the field; the centre multiplies by 1.0, which is exact
       const double fac = (D < p.e1_lo || D > p.e1_hi) ? ((D < p.e2_lo || D > p.e2_hi) ? 0.25 : 0.75) : 1.0;
       return v3(p.F[0] * fac * s * taper, p.F[1] * fac * s * taper, p.F[2] * fac * s * taper);
@@ -162,20 +172,14 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
                    __shfl_sync(full, mine.z, nfields + f));
     }
   };
+  // lanes 0..8 store x, y, z, beta (= v/c) and a/c; selects, not branches, so the warp never diverges
+  const double rC = 1.0 / C;
   auto store = [&](int64_t k, V3 pos, V3 vel, V3 acc) {
-    double v = 0;
-    switch (lane) {
-      case 0: v = pos.x; break;
-      case 1: v = pos.y; break;
-      case 2: v = pos.z; break;
-      case 3: v = vel.x / C; break;
-      case 4: v = vel.y / C; break;
-      case 5: v = vel.z / C; break;
-      case 6: v = acc.x / C; break;
-      case 7: v = acc.y / C; break;
-      case 8: v = acc.z / C; break;
-    }
-    if (out) out[k] = v;
+    const int l3 = lane < 3 ? lane : lane < 6 ? lane - 3 : lane - 6;
+    const V3 src = lane < 3 ? pos : lane < 6 ? vel : acc;
+    const double v = l3 == 0 ? src.x : l3 == 1 ? src.y : src.z;
+    const double q = div_rn(v, C, rC);
+    if (out) out[k] = lane < 3 ? v : q;
   };
   // one RK4 step of size h from (pos, vel); returns the derivative at the start state (its velocity part)
   auto step = [&](V3 &pos, V3 &vel, double h) -> V3 {
@@ -267,10 +271,11 @@ __global__ void __launch_bounds__(64) rk4_thread_kernel(const srs_field *__restr
     vel = nvel;
     return a1;
   };
+  const double rC = 1.0 / C;
   auto store = [&](int64_t k, V3 pos, V3 vel, V3 acc) {
     xp[k] = pos.x; xp[n + k] = pos.y; xp[2 * n + k] = pos.z;
-    bp[k] = vel.x / C; bp[n + k] = vel.y / C; bp[2 * n + k] = vel.z / C;
-    ap[k] = acc.x / C; ap[n + k] = acc.y / C; ap[2 * n + k] = acc.z / C;
+    bp[k] = div_rn(vel.x, C, rC); bp[n + k] = div_rn(vel.y, C, rC); bp[2 * n + k] = div_rn(vel.z, C, rC);
+    ap[k] = div_rn(acc.x, C, rC); ap[n + k] = div_rn(acc.y, C, rC); ap[2 * n + k] = div_rn(acc.z, C, rC);
   };
   const V3 pos0 = v3(P.x0[0], P.x0[1], P.x0[2]);
   const V3 vel0 = v3(P.beta0[0] * C, P.beta0[1] * C, P.beta0[2] * C);

@@ -206,6 +206,19 @@ struct srs_sim {
   std::vector<double *> grid_dev;             // device samples per field (nullptr otherwise)
   double *d_fields = nullptr;                 // device copy of `fields`
   bool fields_dirty = true;
+  uint64_t fields_version = 0;                // bumped by every field change (trajectory cache key)
+  // Device trajectory of the last single-particle calculation.  The reference recomputes the same
+  // trajectory on every call; keeping it lets later calls (other energies, maps, spectra) skip the
+  // RK4 when the particle, the fields and the trajectory settings are unchanged.
+  struct TrajCache {
+    bool valid = false;
+    double key[11] = {0};
+    uint64_t fields_version = 0;
+    double *x = nullptr, *b = nullptr, *a = nullptr;
+    int64_t capacity = 0;
+    srs_traj_view view{};
+  } cache;
+  bool cache_enabled = true;
   std::vector<Beam> beams;
   std::vector<double> weight_sums;
   std::map<std::string, size_t> beam_index;
@@ -215,6 +228,9 @@ struct srs_sim {
     for (double *p : grid_dev)
       if (p) cudaFree(p);
     if (d_fields) cudaFree(d_fields);
+    if (cache.x) cudaFree(cache.x);
+    if (cache.b) cudaFree(cache.b);
+    if (cache.a) cudaFree(cache.a);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -241,6 +257,7 @@ struct srs_sim {
     grid_host.push_back(std::move(host_grid));
     grid_dev.push_back(dev);
     fields_dirty = true;
+    ++fields_version;
     return SRS_OK;
   }
 
@@ -300,9 +317,8 @@ struct srs_sim {
     return SRS_OK;
   }
 
-  // RK4 trajectories of a batch of particles that share t0 (device arrays, layout of srs_trajectory).
-  srs_status trajectories(const Particle *ps, int np, DeviceBuffer &X, DeviceBuffer &B, DeviceBuffer &A,
-                          srs_traj_view &view) {
+  // RK4 trajectories of a batch of particles that share t0 into device arrays (layout of srs_trajectory).
+  srs_status integrate(const Particle *ps, int np, double *X, double *B, double *A, srs_traj_view &view) {
     double dt;
     int64_t nf, nb;
     if (srs_status st = srs_trajectory_counts(ctstart, ctstop, ps[0].t0, npoints, &dt, &nf, &nb)) return st;
@@ -315,21 +331,70 @@ struct srs_sim {
       put(hp[i].beta0, ps[i].b0);
       hp[i].qomg = ps[i].qomg;
     }
-    const size_t bytes = sizeof(double) * 3 * (size_t)n * np;
-    SRS_CUDA(X.alloc(bytes, stream));
-    SRS_CUDA(B.alloc(bytes, stream));
-    SRS_CUDA(A.alloc(bytes, stream));
     DeviceBuffer dp;
     SRS_CUDA(dp.alloc(sizeof(srs_particle) * np, stream));
     SRS_CUDA(cudaMemcpyAsync(dp.ptr, hp.data(), sizeof(srs_particle) * np, cudaMemcpyHostToDevice, stream));
     SRS_CUDA(launch_rk4(reinterpret_cast<const srs_field *>(d_fields), (int)fields.size(), dp.as<srs_particle>(), np,
-                        dt, nf, nb, X.as<double>(), B.as<double>(), A.as<double>(), stream));
-    view.x = X.as<double>();
-    view.beta = B.as<double>();
-    view.aoc = A.as<double>();
+                        dt, nf, nb, X, B, A, stream));
+    view.x = X;
+    view.beta = B;
+    view.aoc = A;
     view.n = n;
     view.nparticles = np;
     view.dt = dt;
+    return SRS_OK;
+  }
+
+  srs_status point_count(const Particle &p, int64_t &n) {
+    double dt;
+    int64_t nf, nb;
+    if (srs_status st = srs_trajectory_counts(ctstart, ctstop, p.t0, npoints, &dt, &nf, &nb)) return st;
+    n = nf + nb;
+    return SRS_OK;
+  }
+
+  // A batch into stream-ordered buffers owned by the caller.
+  srs_status trajectories(const Particle *ps, int np, DeviceBuffer &X, DeviceBuffer &B, DeviceBuffer &A,
+                          srs_traj_view &view) {
+    int64_t n;
+    if (srs_status st = point_count(ps[0], n)) return st;
+    const size_t bytes = sizeof(double) * 3 * (size_t)std::max<int64_t>(n, 1) * np;
+    SRS_CUDA(X.alloc(bytes, stream));
+    SRS_CUDA(B.alloc(bytes, stream));
+    SRS_CUDA(A.alloc(bytes, stream));
+    return integrate(ps, np, X.as<double>(), B.as<double>(), A.as<double>(), view);
+  }
+
+  // The trajectory of one particle, from the cache when nothing it depends on has changed.
+  srs_status single(const Particle &p, srs_traj_view &view) {
+    const double key[11] = {p.x0.x, p.x0.y, p.x0.z, p.b0.x, p.b0.y, p.b0.z, p.qomg, p.t0, ctstart, ctstop,
+                            (double)npoints};
+    if (cache_enabled && cache.valid && cache.fields_version == fields_version && cache.view.n > 0 &&
+        std::memcmp(key, cache.key, sizeof key) == 0) {
+      int64_t n;
+      if (srs_status st = point_count(p, n)) return st;
+      if (n == cache.view.n) {
+        view = cache.view;
+        return SRS_OK;
+      }
+    }
+    cache.valid = false;
+    int64_t n;
+    if (srs_status st = point_count(p, n)) return st;
+    if (n > cache.capacity) {
+      for (double **q : {&cache.x, &cache.b, &cache.a}) {
+        if (*q) cudaFree(*q);
+        *q = nullptr;
+      }
+      cache.capacity = 0;
+      for (double **q : {&cache.x, &cache.b, &cache.a}) SRS_CUDA(cudaMalloc(q, sizeof(double) * 3 * (size_t)n));
+      cache.capacity = n;
+    }
+    if (srs_status st = integrate(&p, 1, cache.x, cache.b, cache.a, cache.view)) return st;
+    std::memcpy(cache.key, key, sizeof key);
+    cache.fields_version = fields_version;
+    cache.valid = cache_enabled;
+    view = cache.view;
     return SRS_OK;
   }
 
@@ -367,7 +432,11 @@ struct srs_sim {
       const int np = (int)(b1 - b0);
       DeviceBuffer X, B, A, vals;
       srs_traj_view view;
-      if (srs_status st = trajectories(&ps[b0], np, X, B, A, view)) return st;
+      if (nparticles == 0) {
+        if (srs_status st = single(ps[b0], view)) return st;
+      } else if (srs_status st = trajectories(&ps[b0], np, X, B, A, view)) {
+        return st;
+      }
       SRS_CUDA(vals.alloc(sizeof(double) * (size_t)nout * np, stream));
       srs_beam_consts bc{ps[b0].q, ps[b0].current};
       if (srs_status st = sum(view, bc, vals.as<double>())) return st;
@@ -524,6 +593,14 @@ srs_status srs_sim_clear_bfields(srs_sim *sim) {
   sim->grid_host.clear();
   sim->grid_dev.clear();
   sim->fields_dirty = true;
+  ++sim->fields_version;
+  return SRS_OK;
+}
+
+srs_status srs_sim_set_trajectory_cache(srs_sim *sim, int32_t enabled) {
+  SIM_GUARD(sim);
+  sim->cache_enabled = enabled != 0;
+  sim->cache.valid = false;
   return SRS_OK;
 }
 
@@ -554,6 +631,7 @@ srs_status srs_sim_set_field_grid_data(srs_sim *sim, int32_t k, const double *da
                            on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, sim->stream));
   SRS_CUDA(cudaStreamSynchronize(sim->stream));
   if (!on_device) std::memcpy(sim->grid_host[k].data(), data, sizeof(double) * cnt);
+  ++sim->fields_version;
   return SRS_OK;
 }
 
@@ -683,12 +761,11 @@ srs_status srs_sim_calculate_trajectory(srs_sim *sim, int64_t *n, double *x, dou
     return SRS_OK;
   }
   if (*n != nf + nb) return fail(SRS_ERR_INVALID, "output size does not match the trajectory");
-  DeviceBuffer X, B, A;
   srs_traj_view v;
-  if (srs_status st = sim->trajectories(&sim->particle, 1, X, B, A, v)) return st;
+  if (srs_status st = sim->single(sim->particle, v)) return st;
   std::vector<double> hx(3 * v.n), hb(3 * v.n);
-  SRS_CUDA(cudaMemcpyAsync(hx.data(), X.ptr, sizeof(double) * 3 * v.n, cudaMemcpyDeviceToHost, sim->stream));
-  SRS_CUDA(cudaMemcpyAsync(hb.data(), B.ptr, sizeof(double) * 3 * v.n, cudaMemcpyDeviceToHost, sim->stream));
+  SRS_CUDA(cudaMemcpyAsync(hx.data(), v.x, sizeof(double) * 3 * v.n, cudaMemcpyDeviceToHost, sim->stream));
+  SRS_CUDA(cudaMemcpyAsync(hb.data(), v.beta, sizeof(double) * 3 * v.n, cudaMemcpyDeviceToHost, sim->stream));
   SRS_CUDA(cudaStreamSynchronize(sim->stream));
   for (int64_t i = 0; i < v.n; ++i)
     for (int c = 0; c < 3; ++c) {
@@ -720,7 +797,7 @@ srs_status srs_sim_calculate_flux(srs_sim *sim, const double *points, int64_t np
   if (nparticles < 0) return fail(SRS_ERR_INVALID, "'nparticles' must be >= 1 (sort of)");
   DeviceBuffer dp;
   const double *d_p = nullptr;
-  if (points) {
+  if (points && !(precision == SRS_PRECISION_MIXED && grid)) {  // the mixed kernel walks the grid itself
     SRS_CUDA(dp.alloc(sizeof(double) * 3 * np, sim->stream));
     SRS_CUDA(cudaMemcpyAsync(dp.ptr, points, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, sim->stream));
     d_p = dp.as<double>();
@@ -738,11 +815,15 @@ srs_status srs_sim_calculate_power_density(srs_sim *sim, const double *points, c
   if (!points || !normals || !out || !comp || np < 1) return fail(SRS_ERR_INVALID, "bad argument");
   if (nparticles < 0) return fail(SRS_ERR_INVALID, "'nparticles' must be >= 1 (sort of)");
   DeviceBuffer dp;
-  SRS_CUDA(dp.alloc(sizeof(double) * 6 * np, sim->stream));
-  SRS_CUDA(cudaMemcpyAsync(dp.ptr, points, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, sim->stream));
-  SRS_CUDA(cudaMemcpyAsync(dp.as<double>() + 3 * np, normals, sizeof(double) * 3 * np, cudaMemcpyHostToDevice,
-                           sim->stream));
-  const double *d_p = dp.as<double>(), *d_n = d_p + 3 * np;
+  const double *d_p = nullptr, *d_n = nullptr;
+  if (!(precision == SRS_PRECISION_MIXED && grid)) {  // the mixed kernel walks the grid itself
+    SRS_CUDA(dp.alloc(sizeof(double) * 6 * np, sim->stream));
+    SRS_CUDA(cudaMemcpyAsync(dp.ptr, points, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, sim->stream));
+    SRS_CUDA(cudaMemcpyAsync(dp.as<double>() + 3 * np, normals, sizeof(double) * 3 * np, cudaMemcpyHostToDevice,
+                             sim->stream));
+    d_p = dp.as<double>();
+    d_n = d_p + 3 * np;
+  }
   cudaStream_t s = sim->stream;
   return sim->run(nparticles, np, out, comp, weighted != 0,
                   [&](const srs_traj_view &v, const srs_beam_consts &bc, double *dv) {
@@ -754,9 +835,8 @@ srs_status srs_sim_calculate_total_power(srs_sim *sim, double *out) {
   SIM_GUARD(sim);
   if (!out) return fail(SRS_ERR_INVALID, "NULL output");
   if (srs_status st = sim->ensure_particle()) return st;
-  DeviceBuffer X, B, A;
   srs_traj_view v;
-  if (srs_status st = sim->trajectories(&sim->particle, 1, X, B, A, v)) return st;
+  if (srs_status st = sim->single(sim->particle, v)) return st;
   srs_beam_consts bc{sim->particle.q, sim->particle.current};
   return srs_total_power(v, bc, &sim->particle.gamma, out, sim->stream);
 }

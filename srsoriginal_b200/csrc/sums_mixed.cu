@@ -91,7 +91,17 @@ struct FluxRec {  // per trajectory point, per tile (FP32 unless noted)
 __global__ void __launch_bounds__(kThreads) flux_mixed_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
                                                               int64_t n, double dt, srs_grid2d g, double omega,
                                                               int64_t chunk, double *__restrict__ partial) {
-  __shared__ float sm[18][kSub];
+  // Per trajectory point i (anchored at the tile centre), five float4 records read as broadcasts:
+  //   r0 = (phase mod 1 turn, k1, k2 [turns per grid step, mod 1], (w/c)/(2 D_c) / 2pi [turns per m^2])
+  //   r1 = (n_c, 1/D_c)
+  //   r2 = ((n_c - bhat) + bhat (1 - |beta|), near-field z term -(c/w) n_cz / D_c^2)
+  //   r3 = (1/(2 D_c), unused x3)
+  // Phases are kept in turns so that the reduction to [-1/2, 1/2) is exact (x - rint(x)).
+  // Terms below FP32 resolution are dropped: the third-order distance term g (|Delta|^2 - g^2)/(2 D_c^2)
+  // (< 1e-7 rad here) and the near-field term's x, y parts (relative size lambda/(2 pi D) times
+  // n_perp, < 1e-10 at 30 m); 1/D_j = (1/D_c)(1 - (D_j - D_c)/D_c) to first order (relative error
+  // ((D_j - D_c)/D_c)^2 < 1e-16).
+  __shared__ float4 sm[4][kSub];
   const int tid = threadIdx.x;
   const int T1 = blockIdx.x / ((g.n2 + kTileB - 1) / kTileB), T2 = blockIdx.x % ((g.n2 + kTileB - 1) / kTileB);
   const int a = tid / kTileB, b = tid % kTileB;
@@ -112,7 +122,8 @@ __global__ void __launch_bounds__(kThreads) flux_mixed_kernel(const double *__re
   const float dd = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
   const float fda = (float)da, fdb = (float)db;
   const double wc = omega / kC;
-  const float cow = (float)(kC / omega);
+  const double inv2pi = 0.15915494309189535;
+  const float two_pi_f = 6.28318530717958647692f;
   double E[6] = {0, 0, 0, 0, 0, 0};
 
   for (int64_t base = i0; base < iend; base += kSub) {
@@ -122,45 +133,42 @@ __global__ void __launch_bounds__(kThreads) flux_mixed_kernel(const double *__re
       const int64_t i = base + tid;
       const Anchor A = make_anchor(Oc, xp, bp, n, i);
       const double tau = dt * (double)i + A.Dc / kC;
-      sm[0][tid] = (float)reduce_2pi(omega * tau);
-      sm[1][tid] = (float)reduce_2pi(wc * (A.nc[0] * g.u1[0] + A.nc[1] * g.u1[1] + A.nc[2] * g.u1[2]));
-      sm[2][tid] = (float)reduce_2pi(wc * (A.nc[0] * g.u2[0] + A.nc[1] * g.u2[1] + A.nc[2] * g.u2[2]));
-      sm[3][tid] = (float)(wc * 0.5 * A.invDc);
-      sm[4][tid] = (float)A.invDc;
-      sm[5][tid] = (float)A.Dc;
-      const double bimc = -(kC / omega) * A.invDc * A.invDc;  // near-field term -i (c/w) n / D^2 at the centre
-      for (int c = 0; c < 3; ++c) {
-        sm[6 + c][tid] = (float)A.nc[c];
-        sm[9 + c][tid] = (float)A.dc[c];
-        sm[12 + c][tid] = (float)(A.bhat[c] * A.omb);
-        sm[15 + c][tid] = (float)(bimc * A.nc[c]);
-      }
+      const double k1 = reduce_2pi(wc * (A.nc[0] * g.u1[0] + A.nc[1] * g.u1[1] + A.nc[2] * g.u1[2]));
+      const double k2 = reduce_2pi(wc * (A.nc[0] * g.u2[0] + A.nc[1] * g.u2[1] + A.nc[2] * g.u2[2]));
+      sm[0][tid] = make_float4((float)(reduce_2pi(omega * tau) * inv2pi), (float)(k1 * inv2pi), (float)(k2 * inv2pi),
+                               (float)(wc * 0.5 * A.invDc * inv2pi));
+      sm[1][tid] = make_float4((float)A.nc[0], (float)A.nc[1], (float)A.nc[2], (float)A.invDc);
+      sm[2][tid] = make_float4((float)(A.dc[0] + A.bhat[0] * A.omb), (float)(A.dc[1] + A.bhat[1] * A.omb),
+                               (float)(A.dc[2] + A.bhat[2] * A.omb),
+                               (float)(-(kC / omega) * A.invDc * A.invDc * A.nc[2]));
+      sm[3][tid] = make_float4((float)(0.5 * A.invDc), 0.f, 0.f, 0.f);
     }
     __syncthreads();
     if (!active) continue;
     float e0 = 0, e1 = 0, e2 = 0, e3 = 0, e4 = 0, e5 = 0;
 #pragma unroll 4
     for (int k = 0; k < cnt; ++k) {
-      const float ncx = sm[6][k], ncy = sm[7][k], ncz = sm[8][k];
-      const float gq = fmaf(ncz, Dl[2], fmaf(ncy, Dl[1], ncx * Dl[0]));
-      const float h = fmaf(-gq, gq, dd);
-      const float invD = sm[4][k];
-      const float q = h * sm[3][k] * fmaf(-gq, invD, 1.0f);      // (w/c)(D_j - D_c - g)
-      const float del = fmaf(q, cow, gq);                          // D_j - D_c
-      const float rinv = __fdividef(1.0f, sm[5][k] + del);
-      float ph = fmaf(sm[1][k], fda, sm[0][k]);
-      ph = fmaf(sm[2][k], fdb, ph) + q;
+      const float4 r0 = sm[0][k], r1 = sm[1][k], r2 = sm[2][k];
+      const float hinv = sm[3][k].x;
+      const float gq = fmaf(r1.z, Dl[2], fmaf(r1.y, Dl[1], r1.x * Dl[0]));  // n_c . Delta
+      const float h = fmaf(-gq, gq, dd);                                    // |Delta|^2 - g^2
+      const float del = fmaf(h, hinv, gq);                                  // D_j - D_c
+      const float t = del * r1.w;
+      const float rinv = fmaf(-t, r1.w, r1.w);                              // 1/D_j
+      float ph = fmaf(r0.y, fda, r0.x);
+      ph = fmaf(r0.z, fdb, ph);
+      ph = fmaf(h, r0.w, ph);                                               // turns
+      const float fr = ph - rintf(ph);
       float sn, cs;
-      __sincosf(reduce_2pi_f(ph), &sn, &cs);
-      // amplitude (beta - n_j)/D_j = -((n_j - bhat) + bhat*omb)/D_j
-      const float dnx = fmaf(-ncx, del, Dl[0]) * rinv, dny = fmaf(-ncy, del, Dl[1]) * rinv, dnz = fmaf(-ncz, del, Dl[2]) * rinv;
-      const float ax = -(sm[9][k] + dnx + sm[12][k]) * rinv;
-      const float ay = -(sm[10][k] + dny + sm[13][k]) * rinv;
-      const float az = -(sm[11][k] + dnz + sm[14][k]) * rinv;
-      const float bx = sm[15][k], by = sm[16][k], bz = sm[17][k];
-      e0 = fmaf(ax, cs, fmaf(-bx, sn, e0)); e1 = fmaf(ax, sn, fmaf(bx, cs, e1));
-      e2 = fmaf(ay, cs, fmaf(-by, sn, e2)); e3 = fmaf(ay, sn, fmaf(by, cs, e3));
-      e4 = fmaf(az, cs, fmaf(-bz, sn, e4)); e5 = fmaf(az, sn, fmaf(bz, cs, e5));
+      __sincosf(fr * two_pi_f, &sn, &cs);
+      // amplitude (beta - n_j)/D_j = -((n_c - bhat + bhat omb) + (Delta - n_c del)/D_j)/D_j
+      const float ux = fmaf(fmaf(-r1.x, del, Dl[0]), rinv, r2.x);
+      const float uy = fmaf(fmaf(-r1.y, del, Dl[1]), rinv, r2.y);
+      const float uz = fmaf(fmaf(-r1.z, del, Dl[2]), rinv, r2.z);
+      const float ax = ux * rinv, ay = uy * rinv, az = uz * rinv;  // minus the amplitude
+      e0 = fmaf(-ax, cs, e0); e1 = fmaf(-ax, sn, e1);
+      e2 = fmaf(-ay, cs, e2); e3 = fmaf(-ay, sn, e3);
+      e4 = fmaf(-az, cs, fmaf(-r2.w, sn, e4)); e5 = fmaf(-az, sn, fmaf(r2.w, cs, e5));
     }
     E[0] += e0; E[1] += e1; E[2] += e2; E[3] += e3; E[4] += e4; E[5] += e5;
   }
@@ -180,7 +188,11 @@ __global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__rest
   // (1 - n.beta)^5 ~ 1e-39 does not fit FP32, so the FP32 term is scaled: with omb = 1 - |beta|,
   // 1 - n.beta = omb_i * opn, opn = 1 + (|beta|/(2 omb_i)) |n - bhat|^2 >= 1, and
   // 1/(1 - n.beta)^5 = (omb_ref/omb_i)^5 / opn^5 / omb_ref^5; the last factor (~1e39) is applied in FP64.
-  __shared__ float sm[18][kSub];
+  // Per trajectory point i, five float4 records read as broadcasts:
+  //   r0 = (n_c, 1/D_c)                 r1 = (n_c - bhat, 1/(2 D_c))
+  //   r2 = (bhat (1 - |beta|), omb_i)   r3 = (a/c, |beta|/(2 omb_i))
+  //   r4 = (bhat . a, (omb_ref/omb_i)^5, n_c . normal, unused)
+  __shared__ float4 sm[5][kSub];
   const int tid = threadIdx.x;
   const int nt2 = (g.n2 + kTileB - 1) / kTileB;
   const int T1 = blockIdx.x / nt2, T2 = blockIdx.x % nt2;
@@ -216,47 +228,43 @@ __global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__rest
       const Anchor A = make_anchor(Oc, xp, bp, n, i);
       const double ax = ap[i], ay = ap[n + i], az = ap[2 * n + i];
       const double r = omb_ref / A.omb;
-      sm[0][tid] = (float)A.invDc;
-      sm[1][tid] = (float)A.Dc;
-      sm[2][tid] = (float)A.omb;
-      sm[3][tid] = (float)(0.5 * A.bmag / A.omb);
-      sm[4][tid] = (float)(A.bhat[0] * ax + A.bhat[1] * ay + A.bhat[2] * az);  // bhat . a
-      for (int c = 0; c < 3; ++c) {
-        sm[5 + c][tid] = (float)A.nc[c];
-        sm[8 + c][tid] = (float)A.dc[c];
-        sm[11 + c][tid] = (float)(A.bhat[c] * A.omb);
-      }
-      sm[14][tid] = (float)ax; sm[15][tid] = (float)ay; sm[16][tid] = (float)az;
-      sm[17][tid] = (float)(r * r * r * r * r);
+      sm[0][tid] = make_float4((float)A.nc[0], (float)A.nc[1], (float)A.nc[2], (float)A.invDc);
+      sm[1][tid] = make_float4((float)A.dc[0], (float)A.dc[1], (float)A.dc[2], (float)(0.5 * A.invDc));
+      sm[2][tid] = make_float4((float)(A.bhat[0] * A.omb), (float)(A.bhat[1] * A.omb), (float)(A.bhat[2] * A.omb),
+                               (float)A.omb);
+      sm[3][tid] = make_float4((float)ax, (float)ay, (float)az, (float)(0.5 * A.bmag / A.omb));
+      sm[4][tid] = make_float4((float)(A.bhat[0] * ax + A.bhat[1] * ay + A.bhat[2] * az), (float)(r * r * r * r * r),
+                               (float)(A.nc[0] * nx_ + A.nc[1] * ny_ + A.nc[2] * nz_), 0.f);
     }
     __syncthreads();
     if (!active) continue;
     float acc = 0;
 #pragma unroll 4
     for (int k = 0; k < cnt; ++k) {
-      const float ncx = sm[5][k], ncy = sm[6][k], ncz = sm[7][k];
-      const float gq = fmaf(ncz, Dl[2], fmaf(ncy, Dl[1], ncx * Dl[0]));
+      const float4 r0 = sm[0][k], r1 = sm[1][k];
+      const float gq = fmaf(r0.z, Dl[2], fmaf(r0.y, Dl[1], r0.x * Dl[0]));  // n_c . Delta
       const float h = fmaf(-gq, gq, dd);
-      const float invD = sm[0][k];
-      const float del = fmaf(0.5f * h * invD, fmaf(-gq, invD, 1.0f), gq);  // D_j - D_c
-      const float rinv = __fdividef(1.0f, sm[1][k] + del);
-      const float dnx = fmaf(-ncx, del, Dl[0]) * rinv, dny = fmaf(-ncy, del, Dl[1]) * rinv, dnz = fmaf(-ncz, del, Dl[2]) * rinv;
-      const float dx = sm[8][k] + dnx, dy = sm[9][k] + dny, dz = sm[10][k] + dnz;  // n_j - bhat
-      const float nx = ncx + dnx, ny = ncy + dny, nz = ncz + dnz;
-      const float nd = fmaf(nz, nrz, fmaf(ny, nry, nx * nrx));
+      const float del = fmaf(h, r1.w, gq);                                    // D_j - D_c
+      const float t = del * r0.w;
+      const float rinv = fmaf(-t, r0.w, r0.w);                                // 1/D_j
+      const float dnx = fmaf(-r0.x, del, Dl[0]) * rinv, dny = fmaf(-r0.y, del, Dl[1]) * rinv,
+                  dnz = fmaf(-r0.z, del, Dl[2]) * rinv;                       // n_j - n_c
+      const float4 r4 = sm[4][k];
+      const float nd = fmaf(dnz, nrz, fmaf(dny, nry, fmaf(dnx, nrx, r4.z)));  // n_j . normal
       if (directional && nd <= 0.0f) continue;
+      const float4 r2 = sm[2][k], r3 = sm[3][k];
+      const float dx = r1.x + dnx, dy = r1.y + dny, dz = r1.z + dnz;           // n_j - bhat
       const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-      const float opn = fmaf(sm[3][k], d2, 1.0f);  // (1 - n.beta) / omb_i
-      const float opnb = sm[2][k] * opn;           // 1 - n.beta
-      const float axx = sm[14][k], ayy = sm[15][k], azz = sm[16][k];
-      const float na = fmaf(dz, azz, fmaf(dy, ayy, fmaf(dx, axx, sm[4][k])));  // n . a
+      const float opn = fmaf(r3.w, d2, 1.0f);  // (1 - n.beta) / omb_i
+      const float opnb = r2.w * opn;           // 1 - n.beta
+      const float na = fmaf(dz, r3.z, fmaf(dy, r3.y, fmaf(dx, r3.x, r4.x)));  // n . a
       // V = n x ((n - beta) x a) = (n - beta)(n.a) - a (1 - n.beta)
-      const float Xx = dx + sm[11][k], Xy = dy + sm[12][k], Xz = dz + sm[13][k];
-      const float Vx = fmaf(Xx, na, -axx * opnb), Vy = fmaf(Xy, na, -ayy * opnb), Vz = fmaf(Xz, na, -azz * opnb);
+      const float Xx = dx + r2.x, Xy = dy + r2.y, Xz = dz + r2.z;
+      const float Vx = fmaf(Xx, na, -r3.x * opnb), Vy = fmaf(Xy, na, -r3.y * opnb), Vz = fmaf(Xz, na, -r3.z * opnb);
       const float v2 = fmaf(Vz, Vz, fmaf(Vy, Vy, Vx * Vx));
       const float o2 = opn * opn;
       const float o5 = o2 * o2 * opn;
-      acc = fmaf(v2 * rinv * rinv * nd * sm[17][k], __fdividef(1.0f, o5), acc);
+      acc = fmaf(v2 * rinv * rinv * nd * r4.y, __fdividef(1.0f, o5), acc);
     }
     sum += (double)acc;
   }

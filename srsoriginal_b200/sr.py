@@ -193,6 +193,12 @@ class sr:  # noqa: N801  (the reference's type name)
     def clear_bfields(self):
         check(lib.srs_sim_clear_bfields(self._h))
 
+    def set_trajectory_cache(self, enabled=True):
+        """Keep (True, the default) or not the device trajectory of the last single-particle call for
+        reuse while the particle, fields and trajectory settings are unchanged; any call drops the
+        kept trajectory."""
+        check(lib.srs_sim_set_trajectory_cache(self._h, 1 if enabled else 0))
+
     # ------------------------------------------------------------ particle beams
     def add_particle_beam(self, type, name, energy_GeV, d0, x0, sigma_energy_GeV=0.0, t0=0.0, current=0.0,
                           weight=1.0, rotations=None, translation=None, horizontal_direction=None, beta=None,
