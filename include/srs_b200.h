@@ -188,6 +188,52 @@ srs_status srs_total_power(srs_traj_view traj, srs_beam_consts beam, const doubl
 srs_status srs_accumulate(const double *d_vals, int32_t nparticles, int64_t nout, double weight,
                           double *out, double *comp, void *stream);
 
+/* ------------------------------------------------------------------ heterogeneous work queue
+ * No counterpart in the reference (which runs one calculation per call, each with its own launch
+ * and host synchronisation, OSCARSSR.cc:1154-1251 and 1989-2099): a set of mixed-precision flux and
+ * spectrum jobs of different sizes, each with its own trajectory, run as ONE persistent launch.
+ * The jobs are cut into (tile, trajectory chunk) work items, ordered longest first; resident CTAs
+ * take items from an atomic ticket.  srs_queue_run replays a CUDA graph captured on its first call
+ * (ticket reset, queue kernel, chunk-order reduction).  Results equal srs_spectrum / srs_flux
+ * (SRS_PRECISION_MIXED, one particle) to rounding of the per-chunk partial sums. */
+enum { SRS_JOB_FLUX = 0, SRS_JOB_SPECTRUM = 1 };
+
+typedef struct srs_job {
+  int32_t kind;          /* SRS_JOB_FLUX or SRS_JOB_SPECTRUM */
+  srs_traj_view traj;    /* one particle (nparticles is ignored); DEVICE arrays */
+  srs_beam_consts beam;
+  srs_grid2d grid;       /* flux: the observation grid */
+  double energy_ev;      /* flux: photon energy */
+  double obs[3];         /* spectrum: observer */
+  const double *d_energies; /* spectrum: DEVICE, ne photon energies [eV], read at srs_queue_create */
+  int64_t ne;
+  double *d_out;         /* DEVICE: n1*n2 (flux) or ne (spectrum) values, weight 1 */
+} srs_job;
+
+typedef struct srs_queue srs_queue;
+
+/* Plan the jobs: chunk = trajectory points per work item (>= 128), ctas_per_sm = resident CTAs per
+ * SM of the persistent grid (0: as many as fit).  The trajectories and outputs must stay valid and
+ * at the same addresses for the queue's lifetime.  Synchronises the device (it reads the
+ * spectrum jobs' energies once). */
+srs_status srs_queue_create(srs_queue **out, const srs_job *jobs, int32_t njobs, int32_t chunk,
+                            int32_t ctas_per_sm);
+/* Run every job once, ordered after the work already queued on stream; later work on stream waits
+ * for the results. */
+srs_status srs_queue_run(srs_queue *q, void *stream);
+/* Work items, field evaluations (points x trajectory points) per run, scratch bytes, CTAs. */
+srs_status srs_queue_info(srs_queue *q, int64_t *nitems, double *evals, size_t *scratch_bytes,
+                          int32_t *grid);
+void srs_queue_destroy(srs_queue *q);
+
+/* RK4 trajectories of nparticles particles with per-particle ctstart/ctstop/t0/npoints (HOST
+ * arrays) in one launch, each written to its own DEVICE arrays d_x[p], d_beta[p], d_aoc[p] (3*n_p
+ * doubles each, layout as srs_trajectory).  Same arithmetic as srs_trajectory. */
+srs_status srs_trajectory_batch(const srs_field *fields, int32_t nfields, const srs_particle *particles,
+                                int32_t nparticles, const double *ctstart, const double *ctstop,
+                                const double *t0, const int64_t *npoints, double *const *d_x,
+                                double *const *d_beta, double *const *d_aoc, void *stream);
+
 /* ------------------------------------------------------------------ simulation object
  * The state and calls behind the reference's Python type oscars.sr.sr (src/OSCARSSR_Python.cc),
  * for the hot-path methods.  One object per thread; calls on one object are serialised. */

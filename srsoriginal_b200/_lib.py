@@ -44,6 +44,15 @@ class Grid2D(C.Structure):
                 ("n2", C.c_int32)]
 
 
+class Job(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("traj", TrajView), ("beam", BeamConsts), ("grid", Grid2D),
+                ("energy_ev", C.c_double), ("obs", _V3), ("d_energies", C.c_void_p), ("ne", C.c_int64),
+                ("d_out", C.c_void_p)]
+
+
+JOB_FLUX, JOB_SPECTRUM = 0, 1
+
+
 class BeamArgs(C.Structure):
     _fields_ = [("type", C.c_char_p), ("name", C.c_char_p), ("energy_gev", C.c_double), ("d0", _V3),
                 ("x0", _V3), ("sigma_energy_gev", C.c_double), ("t0", C.c_double),
@@ -114,6 +123,12 @@ def _load():
         "srs_sim_calculate_total_power": (S, [P, _D]),
         "srs_measure_peak": (S, [C.c_int32, _D, P]),
         "srs_flux_mixed_noalloc": (S, [TrajView, BeamConsts, C.POINTER(Grid2D), C.c_double, P, P]),
+        "srs_queue_create": (S, [C.POINTER(P), C.POINTER(Job), C.c_int32, C.c_int32, C.c_int32]),
+        "srs_queue_run": (S, [P, P]),
+        "srs_queue_info": (S, [P, C.POINTER(C.c_int64), _D, C.POINTER(C.c_size_t), C.POINTER(C.c_int32)]),
+        "srs_queue_destroy": (None, [P]),
+        "srs_trajectory_batch": (S, [C.POINTER(Field), C.c_int32, C.POINTER(Particle), C.c_int32, _D, _D, _D,
+                                     C.POINTER(C.c_int64), C.POINTER(P), C.POINTER(P), C.POINTER(P), P]),
         "srs_energy_grid": (S, [C.c_int64, C.c_double, C.c_double, _D]),
         "srs_rectangle_plane": (S, [C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_double, _D, _D,
                                     C.c_int32, _D, _D, _D, C.POINTER(Grid2D)]),
@@ -141,7 +156,8 @@ EXPORTED = (
     "srs_sim_get_particle srs_set_seed srs_random_uniform srs_random_normal srs_random_reset "
     "srs_sim_calculate_trajectory srs_sim_calculate_spectrum srs_sim_calculate_flux "
     "srs_sim_calculate_power_density srs_sim_calculate_total_power srs_energy_grid "
-    "srs_rectangle_plane srs_rectangle_points srs_measure_peak srs_flux_mixed_noalloc"
+    "srs_rectangle_plane srs_rectangle_points srs_measure_peak srs_flux_mixed_noalloc "
+    "srs_queue_create srs_queue_run srs_queue_info srs_queue_destroy srs_trajectory_batch"
 ).split()
 
 

@@ -27,6 +27,7 @@ SOURCES = [
     ("rk4.cu", True),
     ("sums_fp64.cu", True),
     ("sums_mixed.cu", False),
+    ("queue.cu", False),
     ("capi.cu", True),
     ("sim.cpp", True),
     ("peaks.cu", False),

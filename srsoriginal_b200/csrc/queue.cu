@@ -1,0 +1,312 @@
+// Heterogeneous jobs in one persistent launch: a work queue of (job, tile, trajectory chunk) items.
+//
+// Jobs of very different sizes (a 64-point map next to a 40401-point one, 100 energies next to 4000,
+// trajectories of 5001 to 40001 points) are cut into items of the same shape as the one-shot mixed
+// kernels' CTAs -- a tile of 8 x 16 grid points or 512 energies against one chunk of the trajectory.
+// The host orders the items by decreasing cost (longest-processing-time first), and a grid of
+// resident CTAs (one wave: SMs x CTAs per SM) drains them: each CTA takes the next item with one
+// atomicAdd on a ticket and runs it.  No CTA waits on another (no spin), so the launch always ends.
+// A second kernel adds every job's per-chunk partial sums in chunk order and writes the flux.
+//
+// The launch sequence (ticket reset, queue kernel, finishing kernel) is captured once into a CUDA
+// graph on the queue's own stream and replayed by every srs_queue_run; the caller's stream is joined
+// with events on both sides.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <numeric>
+#include <vector>
+
+#include "mixed_tiles.cuh"
+#include "srs_device.cuh"
+#include "srs_internal.h"
+
+namespace srs {
+namespace {
+
+using namespace tiles;
+
+struct QJob {
+  int kind;
+  int t2;          // flux: tiles along n2
+  int64_t chunk;   // trajectory points per item
+  const double *x, *beta;
+  int64_t n;
+  double dt;
+  double omega;    // flux
+  srs_grid2d g;    // flux
+  V3 obs;          // spectrum
+  const double *omegas;  // spectrum (device, ne)
+  int64_t ne;
+  double *partial;  // nchunks x 6 x nout
+  int64_t nout;
+  int nchunks;
+  double C0, C2;
+  double *out;
+};
+
+struct QItem {
+  int job, tile, chunk, pad;
+};
+
+__global__ void __launch_bounds__(kThreads) queue_kernel(const QJob *__restrict__ jobs, const QItem *__restrict__ items,
+                                                         int nitems, unsigned int *__restrict__ ticket) {
+  __shared__ union {
+    FluxShared f;
+    SpecShared s;
+  } sh;
+  __shared__ int cur;
+  for (;;) {
+    __syncthreads();  // every thread is done with the previous item (and with `cur`)
+    if (threadIdx.x == 0) cur = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int it = cur;
+    if (it >= nitems) return;  // uniform across the CTA
+    const QItem w = items[it];
+    const QJob &J = jobs[w.job];
+    const int64_t i0 = (int64_t)w.chunk * J.chunk, i1 = imin64(J.n, i0 + J.chunk);
+    double *out6 = J.partial + (int64_t)w.chunk * 6 * J.nout;
+    if (J.kind == SRS_JOB_FLUX)
+      flux_tile(J.x, J.beta, J.n, J.dt, J.g, J.omega, w.tile / J.t2, w.tile % J.t2, i0, i1, out6, sh.f);
+    else
+      spectrum_tile(J.x, J.beta, J.n, J.dt, J.obs, J.omegas, J.ne, w.tile, i0, i1, out6, sh.s);
+  }
+}
+
+// out[o] of every job: the chunk partials added in chunk order, then the reference's final scaling.
+__global__ void queue_finish(const QJob *__restrict__ jobs, int njobs, const int64_t *__restrict__ offsets,
+                             int64_t total) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  int lo = 0, hi = njobs - 1;  // job with offsets[job] <= idx < offsets[job + 1]
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (offsets[mid] <= idx) lo = mid;
+    else hi = mid - 1;
+  }
+  const QJob &J = jobs[lo];
+  const int64_t o = idx - offsets[lo];
+  double e[6] = {0, 0, 0, 0, 0, 0};
+  for (int s = 0; s < J.nchunks; ++s) {
+    const double *p = J.partial + (int64_t)s * 6 * J.nout + o;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) e[c] += p[c * J.nout];
+  }
+  const double omega = J.kind == SRS_JOB_FLUX ? J.omega : J.omegas[o];
+  J.out[o] = finish_flux(e, omega, J.dt, J.C0, J.C2);
+}
+
+__global__ void omegas_of(const double *__restrict__ e, int64_t ne, double *__restrict__ w) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ne) w[i] = ev_to_omega(e[i]);
+}
+
+}  // namespace
+}  // namespace srs
+
+using namespace srs;
+
+struct srs_queue {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  QJob *d_jobs = nullptr;
+  QItem *d_items = nullptr;
+  int64_t *d_offsets = nullptr;
+  unsigned int *d_ticket = nullptr;
+  double *d_scratch = nullptr;  // partials, then the spectrum jobs' angular frequencies
+  int njobs = 0, nitems = 0, grid = 0;
+  int64_t total_out = 0;
+  double evals = 0;
+  size_t scratch_bytes = 0;
+
+  ~srs_queue() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void *p : {(void *)d_jobs, (void *)d_items, (void *)d_offsets, (void *)d_ticket, (void *)d_scratch})
+      if (p) cudaFree(p);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+extern "C" {
+
+srs_status srs_queue_create(srs_queue **out, const srs_job *jobs, int32_t njobs, int32_t chunk,
+                            int32_t ctas_per_sm) {
+  clear_error();
+  if (!out || !jobs || njobs < 1) return fail(SRS_ERR_INVALID, "no jobs");
+  if (chunk < 128) return fail(SRS_ERR_INVALID, "chunk must be >= 128 trajectory points");
+  std::unique_ptr<srs_queue> q(new srs_queue());
+  std::vector<QJob> hj(njobs);
+  std::vector<int64_t> offsets(njobs + 1, 0);
+  size_t scratch = 0, omega_doubles = 0;
+  struct Cost {
+    double cost;
+    QItem item;
+  };
+  std::vector<Cost> items;
+  for (int j = 0; j < njobs; ++j) {
+    const srs_job &s = jobs[j];
+    if (!s.traj.x || !s.traj.beta || s.traj.n < 1 || !(s.traj.dt > 0) || !s.d_out)
+      return fail(SRS_ERR_INVALID, "job " + std::to_string(j) + ": bad trajectory or output");
+    QJob &J = hj[j];
+    std::memset(&J, 0, sizeof J);
+    J.kind = s.kind;
+    J.chunk = chunk;
+    J.x = s.traj.x;
+    J.beta = s.traj.beta;
+    J.n = s.traj.n;
+    J.dt = s.traj.dt;
+    J.C0 = flux_c0(s.beam.charge);
+    J.C2 = flux_c2(s.beam.charge, s.beam.current);
+    J.out = s.d_out;
+    J.nchunks = (int)((s.traj.n + chunk - 1) / chunk);
+    int ntiles;
+    double per_item;
+    if (s.kind == SRS_JOB_FLUX) {
+      if (s.grid.n1 < 1 || s.grid.n2 < 1 || !(s.energy_ev > 0))
+        return fail(SRS_ERR_INVALID, "job " + std::to_string(j) + ": bad flux grid or energy");
+      J.g = s.grid;
+      J.omega = ev_to_omega(s.energy_ev);
+      J.t2 = (s.grid.n2 + kTileB - 1) / kTileB;
+      ntiles = ((s.grid.n1 + kTileA - 1) / kTileA) * J.t2;
+      J.nout = (int64_t)s.grid.n1 * s.grid.n2;
+      per_item = kTileA * kTileB;
+      q->evals += (double)J.nout * s.traj.n;
+    } else if (s.kind == SRS_JOB_SPECTRUM) {
+      if (s.ne < 1 || !s.d_energies) return fail(SRS_ERR_INVALID, "job " + std::to_string(j) + ": no energies");
+      J.obs = v3(s.obs[0], s.obs[1], s.obs[2]);
+      J.ne = s.ne;
+      J.nout = s.ne;
+      ntiles = (int)((s.ne + kThreads * kEnergiesPerThread - 1) / (kThreads * kEnergiesPerThread));
+      per_item = 0.6 * kThreads * kEnergiesPerThread;  // a uniform-grid energy costs ~0.6 of a map point
+      omega_doubles += s.ne;
+      q->evals += (double)J.nout * s.traj.n;
+    } else {
+      return fail(SRS_ERR_INVALID, "job " + std::to_string(j) + ": unknown kind");
+    }
+    scratch += (size_t)J.nchunks * 6 * J.nout;
+    offsets[j + 1] = offsets[j] + J.nout;
+    for (int t = 0; t < ntiles; ++t)
+      for (int c = 0; c < J.nchunks; ++c) {
+        const double len = (double)(std::min<int64_t>(s.traj.n, (int64_t)(c + 1) * chunk) - (int64_t)c * chunk);
+        items.push_back(Cost{per_item * len, QItem{j, t, c, 0}});
+      }
+  }
+  if (items.size() > (size_t)0x7fffffff) return fail(SRS_ERR_RANGE, "too many work items");
+  std::stable_sort(items.begin(), items.end(), [](const Cost &a, const Cost &b) { return a.cost > b.cost; });
+  std::vector<QItem> hi(items.size());
+  for (size_t i = 0; i < items.size(); ++i) hi[i] = items[i].item;
+  q->njobs = njobs;
+  q->nitems = (int)items.size();
+  q->total_out = offsets[njobs];
+  q->scratch_bytes = sizeof(double) * (scratch + omega_doubles);
+  SRS_CUDA(cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking));
+  SRS_CUDA(cudaEventCreateWithFlags(&q->ev_in, cudaEventDisableTiming));
+  SRS_CUDA(cudaEventCreateWithFlags(&q->ev_out, cudaEventDisableTiming));
+  SRS_CUDA(cudaMalloc(&q->d_scratch, q->scratch_bytes));
+  SRS_CUDA(cudaDeviceSynchronize());  // the energies may still be being written on the caller's stream
+  // carve partials and angular frequencies
+  size_t off = 0;
+  for (int j = 0; j < njobs; ++j) {
+    hj[j].partial = q->d_scratch + off;
+    off += (size_t)hj[j].nchunks * 6 * hj[j].nout;
+  }
+  for (int j = 0; j < njobs; ++j)
+    if (hj[j].kind == SRS_JOB_SPECTRUM) {
+      double *w = q->d_scratch + off;
+      omegas_of<<<(unsigned)((hj[j].ne + 255) / 256), 256, 0, q->stream>>>(jobs[j].d_energies, hj[j].ne, w);
+      SRS_CUDA(cudaGetLastError());
+      hj[j].omegas = w;
+      off += hj[j].ne;
+    }
+  SRS_CUDA(cudaMalloc(&q->d_jobs, sizeof(QJob) * njobs));
+  SRS_CUDA(cudaMalloc(&q->d_items, sizeof(QItem) * std::max<size_t>(1, hi.size())));
+  SRS_CUDA(cudaMalloc(&q->d_offsets, sizeof(int64_t) * (njobs + 1)));
+  SRS_CUDA(cudaMalloc(&q->d_ticket, sizeof(unsigned int)));
+  SRS_CUDA(cudaMemcpyAsync(q->d_jobs, hj.data(), sizeof(QJob) * njobs, cudaMemcpyHostToDevice, q->stream));
+  SRS_CUDA(cudaMemcpyAsync(q->d_items, hi.data(), sizeof(QItem) * hi.size(), cudaMemcpyHostToDevice, q->stream));
+  SRS_CUDA(cudaMemcpyAsync(q->d_offsets, offsets.data(), sizeof(int64_t) * (njobs + 1), cudaMemcpyHostToDevice,
+                           q->stream));
+  SRS_CUDA(cudaStreamSynchronize(q->stream));
+  int dev = 0, sms = 0, occ = 0;
+  SRS_CUDA(cudaGetDevice(&dev));
+  SRS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SRS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, queue_kernel, kThreads, 0));
+  const int per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, std::max(1, occ)) : std::max(1, occ);
+  q->grid = std::max(1, std::min(sms * per_sm, q->nitems));
+  *out = q.release();
+  return SRS_OK;
+}
+
+srs_status srs_queue_run(srs_queue *q, void *stream) {
+  clear_error();
+  if (!q) return fail(SRS_ERR_INVALID, "NULL queue");
+  cudaStream_t caller = static_cast<cudaStream_t>(stream);
+  SRS_CUDA(cudaEventRecord(q->ev_in, caller));
+  SRS_CUDA(cudaStreamWaitEvent(q->stream, q->ev_in, 0));
+  if (!q->exec) {
+    SRS_CUDA(cudaStreamBeginCapture(q->stream, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(q->d_ticket, 0, sizeof(unsigned int), q->stream);
+    queue_kernel<<<q->grid, kThreads, 0, q->stream>>>(q->d_jobs, q->d_items, q->nitems, q->d_ticket);
+    queue_finish<<<(unsigned)((q->total_out + 255) / 256), 256, 0, q->stream>>>(q->d_jobs, q->njobs, q->d_offsets,
+                                                                                 q->total_out);
+    cudaError_t launch = cudaGetLastError();
+    cudaError_t end = cudaStreamEndCapture(q->stream, &q->graph);
+    if (launch != cudaSuccess) return cuda_fail(launch, "capture of the queue launches");
+    if (end != cudaSuccess) return cuda_fail(end, "cudaStreamEndCapture");
+    SRS_CUDA(cudaGraphInstantiate(&q->exec, q->graph, 0));
+  }
+  SRS_CUDA(cudaGraphLaunch(q->exec, q->stream));
+  SRS_CUDA(cudaEventRecord(q->ev_out, q->stream));
+  SRS_CUDA(cudaStreamWaitEvent(caller, q->ev_out, 0));
+  return SRS_OK;
+}
+
+srs_status srs_queue_info(srs_queue *q, int64_t *nitems, double *evals, size_t *scratch_bytes, int32_t *grid) {
+  clear_error();
+  if (!q) return fail(SRS_ERR_INVALID, "NULL queue");
+  if (nitems) *nitems = q->nitems;
+  if (evals) *evals = q->evals;
+  if (scratch_bytes) *scratch_bytes = q->scratch_bytes;
+  if (grid) *grid = q->grid;
+  return SRS_OK;
+}
+
+void srs_queue_destroy(srs_queue *q) { delete q; }
+
+srs_status srs_trajectory_batch(const srs_field *fields, int32_t nfields, const srs_particle *particles,
+                                int32_t nparticles, const double *ctstart, const double *ctstop, const double *t0,
+                                const int64_t *npoints, double *const *d_x, double *const *d_beta,
+                                double *const *d_aoc, void *stream) {
+  clear_error();
+  if (nparticles < 1 || !particles || !ctstart || !ctstop || !t0 || !npoints || !d_x || !d_beta || !d_aoc)
+    return fail(SRS_ERR_INVALID, "bad argument");
+  if (nfields < 0 || (nfields > 0 && !fields)) return fail(SRS_ERR_INVALID, "bad field array");
+  std::vector<TrajSpec> specs(nparticles);
+  for (int p = 0; p < nparticles; ++p) {
+    double dt;
+    int64_t nf, nb;
+    if (srs_status st = srs_trajectory_counts(ctstart[p], ctstop[p], t0[p], npoints[p], &dt, &nf, &nb)) return st;
+    if (!d_x[p] || !d_beta[p] || !d_aoc[p]) return fail(SRS_ERR_INVALID, "NULL output pointer");
+    specs[p] = TrajSpec{dt, nf, nb, d_x[p], d_beta[p], d_aoc[p]};
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DeviceBuffer df, dp, ds;
+  SRS_CUDA(df.alloc(sizeof(srs_field) * std::max(1, nfields), s));
+  SRS_CUDA(dp.alloc(sizeof(srs_particle) * nparticles, s));
+  SRS_CUDA(ds.alloc(sizeof(TrajSpec) * nparticles, s));
+  if (nfields > 0) SRS_CUDA(cudaMemcpyAsync(df.ptr, fields, sizeof(srs_field) * nfields, cudaMemcpyHostToDevice, s));
+  SRS_CUDA(cudaMemcpyAsync(dp.ptr, particles, sizeof(srs_particle) * nparticles, cudaMemcpyHostToDevice, s));
+  SRS_CUDA(cudaMemcpyAsync(ds.ptr, specs.data(), sizeof(TrajSpec) * nparticles, cudaMemcpyHostToDevice, s));
+  SRS_CUDA(launch_rk4_specs(df.as<srs_field>(), nfields, dp.as<srs_particle>(), ds.as<TrajSpec>(), nparticles, s));
+  return SRS_OK;
+}
+
+}  // extern "C"

@@ -134,11 +134,18 @@ __device__ inline V3 vadd_scaled(V3 a, double h, V3 b) { return v3(a.x + h * b.x
 
 // ---------------------------------------------------------------- warp-cooperative kernel
 
+// A group of G lanes (G = the power of two >= 2 * nfields) owns one particle; a warp holds 32/G
+// particles.  Lane (slot, field) of a group evaluates one field at one of the two positions of a
+// round; groups past the last particle recompute the last one and store nothing, so every lane stays
+// in the shuffles.
+// With specs != nullptr each particle has its own time step, point counts and output arrays (jobs of
+// different trajectory lengths); a warp then runs its longest particle's step count, and groups whose
+// trajectory is complete keep stepping without storing.
 __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restrict__ gfields, int nfields,
                                                        const srs_particle *__restrict__ particles, int nparticles,
-                                                       double dt, int64_t nfwd, int64_t nbwd,
+                                                       double dt_all, int64_t nfwd_all, int64_t nbwd_all, int G,
                                                        double *__restrict__ X, double *__restrict__ Bt,
-                                                       double *__restrict__ A) {
+                                                       double *__restrict__ A, const TrajSpec *__restrict__ specs) {
   __shared__ srs_field sf[kMaxFieldsShared];
   __shared__ Prepared sp[kMaxFieldsShared];
   for (int i = threadIdx.x; i < nfields; i += blockDim.x) {
@@ -147,15 +154,23 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (p >= nparticles) return;  // whole warps exit together
+  const int gl = lane & (G - 1), gbase = lane - gl;
+  const int pp = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 / G) + lane / G;
+  const bool owner = pp < nparticles;
+  const int p = owner ? pp : nparticles - 1;
   const srs_particle P = particles[p];
+  const double dt = specs ? specs[p].dt : dt_all;
+  const int64_t nfwd = specs ? specs[p].nfwd : nfwd_all, nbwd = specs ? specs[p].nbwd : nbwd_all;
   const int64_t n = nfwd + nbwd;
-  double *out = nullptr;  // this lane's output component (lanes 0..8)
-  if (lane < 3) out = X + (int64_t)p * 3 * n + lane * n;
-  else if (lane < 6) out = Bt + (int64_t)p * 3 * n + (lane - 3) * n;
-  else if (lane < 9) out = A + (int64_t)p * 3 * n + (lane - 6) * n;
-  const int slot = nfields > 0 ? lane / nfields : 2, fidx = nfields > 0 ? lane % nfields : 0;
+  double *const xp = specs ? specs[p].x : X + (int64_t)p * 3 * n;
+  double *const bp = specs ? specs[p].beta : Bt + (int64_t)p * 3 * n;
+  double *const ap = specs ? specs[p].aoc : A + (int64_t)p * 3 * n;
+  int64_t fmax = nfwd, bmax = nbwd;  // the warp's longest forward / backward runs
+  for (int o = 16; o > 0; o >>= 1) {
+    fmax = max(fmax, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)fmax, o));
+    bmax = max(bmax, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)bmax, o));
+  }
+  const int slot = nfields > 0 ? gl / nfields : 2, fidx = nfields > 0 ? gl % nfields : 0;
   const bool evaluates = slot < 2;
   const double C = kC, qomg = P.qomg;
   const unsigned full = 0xffffffffu;
@@ -167,19 +182,23 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
     Ba = v3(0, 0, 0);
     Bb = v3(0, 0, 0);
     for (int f = 0; f < nfields; ++f) {
-      Ba = Ba + v3(__shfl_sync(full, mine.x, f), __shfl_sync(full, mine.y, f), __shfl_sync(full, mine.z, f));
-      Bb = Bb + v3(__shfl_sync(full, mine.x, nfields + f), __shfl_sync(full, mine.y, nfields + f),
-                   __shfl_sync(full, mine.z, nfields + f));
+      const int la = gbase + f, lb = gbase + nfields + f;
+      Ba = Ba + v3(__shfl_sync(full, mine.x, la), __shfl_sync(full, mine.y, la), __shfl_sync(full, mine.z, la));
+      Bb = Bb + v3(__shfl_sync(full, mine.x, lb), __shfl_sync(full, mine.y, lb), __shfl_sync(full, mine.z, lb));
     }
   };
-  // lanes 0..8 store x, y, z, beta (= v/c) and a/c; selects, not branches, so the warp never diverges
+  // the group's lanes store the nine components of a point (x, y, z, beta = v/c, a/c), lane gl taking
+  // components gl, gl + G, ...; selects, not branches
   const double rC = 1.0 / C;
   auto store = [&](int64_t k, V3 pos, V3 vel, V3 acc) {
-    const int l3 = lane < 3 ? lane : lane < 6 ? lane - 3 : lane - 6;
-    const V3 src = lane < 3 ? pos : lane < 6 ? vel : acc;
-    const double v = l3 == 0 ? src.x : l3 == 1 ? src.y : src.z;
-    const double q = div_rn(v, C, rC);
-    if (out) out[k] = lane < 3 ? v : q;
+    if (!owner) return;
+    for (int c = gl; c < 9; c += G) {
+      const int l3 = c < 3 ? c : c < 6 ? c - 3 : c - 6;
+      const V3 src = c < 3 ? pos : c < 6 ? vel : acc;
+      const double v = l3 == 0 ? src.x : l3 == 1 ? src.y : src.z;
+      double *const o = (c < 3 ? xp : c < 6 ? bp : ap) + (int64_t)l3 * n + k;
+      *o = c < 3 ? v : div_rn(v, C, rC);
+    }
   };
   // one RK4 step of size h from (pos, vel); returns the derivative at the start state (its velocity part)
   auto step = [&](V3 &pos, V3 &vel, double h) -> V3 {
@@ -212,16 +231,16 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   const V3 pos0 = v3(P.x0[0], P.x0[1], P.x0[2]);
   const V3 vel0 = v3(P.beta0[0] * C, P.beta0[1] * C, P.beta0[2] * C);
   V3 pos = pos0, vel = vel0, acc = v3(0, 0, 0);
-  for (int64_t i = 0; i < nfwd; ++i) {
-    store(nbwd + i, pos, vel, acc);
+  for (int64_t i = 0; i < fmax; ++i) {
+    if (i < nfwd) store(nbwd + i, pos, vel, acc);
     acc = step(pos, vel, dt);
   }
   pos = pos0;
   vel = vel0;
   const double mdt = -dt;
-  for (int64_t i = 0; i < nbwd; ++i) {
+  for (int64_t i = 0; i < bmax; ++i) {
     acc = step(pos, vel, mdt);
-    store(nbwd - 1 - i, pos, vel, acc);
+    if (i < nbwd) store(nbwd - 1 - i, pos, vel, acc);
   }
 }
 
@@ -304,21 +323,47 @@ __global__ void field_eval_kernel(const srs_field *__restrict__ fields, int nfie
 
 }  // namespace
 
+// Lanes per particle: at least 2 * nfields (two positions per round, one field per lane), rounded
+// up to a power of two; then as many as keep the warps at <= 16 per SM, since wider groups store a
+// point's nine components in parallel and shorten the per-step chain, while narrower groups serve
+// more particles per instruction once there are enough particles to fill the SMs.
+static int group_size(int nparticles, int nfields) {
+  int G = 2;
+  while (G < 2 * nfields) G *= 2;
+  while (G < 32 && (int64_t)nparticles * (2 * G) <= (int64_t)148 * 16 * 32) G *= 2;
+  return G;
+}
+
 cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
                        double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
                        cudaStream_t s) {
   if (nparticles <= 0) return cudaSuccess;
   if (nfields > kMaxFieldsShared) return cudaErrorInvalidValue;
-  if (2 * nfields <= 32 && nparticles <= 16384) {
-    const int warps = 4;
-    rk4_warp_kernel<<<(nparticles + warps - 1) / warps, 32 * warps, 0, s>>>(d_fields, nfields, d_particles,
-                                                                            nparticles, dt, nfwd, nbwd, d_x, d_b, d_a);
+  const int G = group_size(nparticles, nfields);
+  // grouped lanes while there are few particles per SM (the serial chain is the limit); one thread
+  // per particle when there are enough particles to fill the SMs (issue rate is the limit)
+  if (G <= 32 && (int64_t)nparticles * G <= 148 * 32 * 48) {
+    const int warps = 4, per_block = warps * (32 / G);
+    rk4_warp_kernel<<<(nparticles + per_block - 1) / per_block, 32 * warps, 0, s>>>(
+        d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, G, d_x, d_b, d_a, nullptr);
   } else {
     const int threads = 64;
     rk4_thread_kernel<<<(nparticles + threads - 1) / threads, threads, 0, s>>>(d_fields, nfields, d_particles,
                                                                                nparticles, dt, nfwd, nbwd, d_x, d_b,
                                                                                d_a);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rk4_specs(const srs_field *d_fields, int nfields, const srs_particle *d_particles,
+                             const TrajSpec *d_specs, int nparticles, cudaStream_t s) {
+  if (nparticles <= 0) return cudaSuccess;
+  if (nfields > kMaxFieldsShared) return cudaErrorInvalidValue;
+  const int G = group_size(nparticles, nfields);
+  if (G > 32) return cudaErrorInvalidValue;
+  const int warps = 4, per_block = warps * (32 / G);
+  rk4_warp_kernel<<<(nparticles + per_block - 1) / per_block, 32 * warps, 0, s>>>(
+      d_fields, nfields, d_particles, nparticles, 0.0, 0, 0, G, nullptr, nullptr, nullptr, d_specs);
   return cudaGetLastError();
 }
 

@@ -194,6 +194,20 @@ __device__ inline V3 field_sum(const srs_field *fields, int nfields, V3 X) {
   return s;
 }
 
+// C2 |SumE * (0 + i C0 w dt)|^2 with libstdc++ complex arithmetic (OSCARSSR.cc:1241-1245); e holds
+// Re/Im of SumE's x, y, z components.
+__device__ inline double finish_flux(const double e[6], double omega, double dt, double C0, double C2) {
+  const double g = (C0 * omega) * dt, z = 0.0 * dt;
+  double parts[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double a = e[2 * c], b = e[2 * c + 1];
+    const double pr = a * z - b * g, pi = a * g + b * z;
+    parts[c] = pr * pr - pi * (-pi);
+  }
+  return C2 * ((parts[0] + parts[1]) + parts[2]);
+}
+
 // ---- phase reduction ----
 // Cody-Waite additive reduction (Cody & Waite, "Software Manual for the Elementary Functions", 1980)
 // of x modulo 2*pi with a three-part 2*pi (P1 + P2 + P3 = 2*pi to ~160 bits; P1, P2 are the double

@@ -46,10 +46,19 @@ struct DeviceBuffer {
   template <class T> T *as() const { return static_cast<T *>(ptr); }
 };
 
+// Per-particle trajectory parameters for batches of different lengths (device array).
+struct TrajSpec {
+  double dt;
+  int64_t nfwd, nbwd;
+  double *x, *beta, *aoc;  // 3 * (nfwd + nbwd) doubles each, [component][point]
+};
+
 // ---- kernel launchers ----
 cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
                        double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
                        cudaStream_t s);
+cudaError_t launch_rk4_specs(const srs_field *d_fields, int nfields, const srs_particle *d_particles,
+                             const TrajSpec *d_specs, int nparticles, cudaStream_t s);
 cudaError_t launch_field_eval(const srs_field *d_fields, int nfields, const double *d_xyz, int64_t np,
                               double *d_out, cudaStream_t s);
 

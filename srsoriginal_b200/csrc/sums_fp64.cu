@@ -88,18 +88,6 @@ __global__ void __launch_bounds__(kTile) flux_fp64_kernel(const double *__restri
   }
 }
 
-// |SumE * (0 + i C0 w dt)|^2 * C2 with libstdc++ complex arithmetic (OSCARSSR.cc:1241-1245).
-__device__ inline double finish_flux(const double e[6], double omega, double dt, double C0, double C2) {
-  const double g = (C0 * omega) * dt, z = 0.0 * dt;
-  double parts[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    double a = e[2 * c], b = e[2 * c + 1];
-    double pr = a * z - b * g, pi = a * g + b * z;
-    parts[c] = pr * pr - pi * (-pi);
-  }
-  return C2 * ((parts[0] + parts[1]) + parts[2]);
-}
 
 __global__ void flux_fp64_reduce(const double *__restrict__ partial, int S, int64_t np, int nparticles,
                                  const double *__restrict__ omegas, double omega0, double dt, double C0, double C2,

@@ -1,0 +1,172 @@
+"""Heterogeneous job queue: many flux-map and spectrum jobs, each with its own trajectory, run as ONE
+persistent launch (srs_queue_*), replayed from a CUDA graph, with an autotuner for the work-item shape.
+
+The reference runs such a set as separate calls (``calculate_spectrum`` / ``calculate_flux_rectangle``
+per job, OSCARSSR_Python.cc:2232 and :3033), each with its own launches and host synchronisation.  Here
+the jobs are cut into work items of one shape -- a tile of 8 x 16 grid points or 512 energies against
+``chunk`` trajectory points -- ordered longest first and drained by resident CTAs from an atomic
+ticket.  The tunable shape is (chunk, CTAs per SM); :func:`autotune` times the candidates on the jobs
+themselves and caches the winner per job-set signature and device in a JSON file.
+
+All tensors are CUDA tensors; every call is ordered on torch's current stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import hashlib
+import json
+import os
+
+import numpy as np
+
+from . import _lib, device
+from ._lib import check, lib
+
+CHUNKS = (1024, 2048, 4096, 8192)
+CTAS_PER_SM = (1, 2, 3, 0)  # 0: as many as fit
+
+
+def flux_job(traj, charge, current, grid, energy_ev, out):
+    """A flux map job: particle 0 of ``traj`` (device.Trajectory) on ``grid`` (srs_grid2d) at one energy;
+    ``out``: CUDA float64 tensor of grid.n1 * grid.n2 values."""
+    j = _lib.Job()
+    j.kind = _lib.JOB_FLUX
+    j.traj = traj.view()
+    j.beam = _lib.BeamConsts(charge, current)
+    j.grid = grid
+    j.energy_ev = float(energy_ev)
+    j.d_out = out.data_ptr()
+    return j, (traj, out)
+
+
+def spectrum_job(traj, charge, current, obs, energies, out):
+    """A spectrum job: particle 0 of ``traj`` at observer ``obs``; ``energies``, ``out``: CUDA float64."""
+    j = _lib.Job()
+    j.kind = _lib.JOB_SPECTRUM
+    j.traj = traj.view()
+    j.beam = _lib.BeamConsts(charge, current)
+    j.obs = _lib.v3(obs)
+    j.d_energies = energies.data_ptr()
+    j.ne = energies.numel()
+    j.d_out = out.data_ptr()
+    return j, (traj, energies, out)
+
+
+class JobQueue:
+    """The planned queue of a list of jobs (from :func:`flux_job` / :func:`spectrum_job`)."""
+
+    def __init__(self, jobs, chunk=2048, ctas_per_sm=0):
+        self._keep = [k for _, k in jobs]  # the tensors must outlive the queue
+        arr = (_lib.Job * len(jobs))(*[j for j, _ in jobs])
+        self._q = C.c_void_p()
+        check(lib.srs_queue_create(C.byref(self._q), arr, len(jobs), int(chunk), int(ctas_per_sm)))
+        self.chunk, self.ctas_per_sm = int(chunk), int(ctas_per_sm)
+        n, ev, sb, g = C.c_int64(), C.c_double(), C.c_size_t(), C.c_int32()
+        check(lib.srs_queue_info(self._q, C.byref(n), C.byref(ev), C.byref(sb), C.byref(g)))
+        self.nitems, self.evals, self.scratch_bytes, self.grid = n.value, ev.value, sb.value, g.value
+
+    def run(self):
+        check(lib.srs_queue_run(self._q, device._stream()))
+
+    def close(self):
+        if self._q:
+            lib.srs_queue_destroy(self._q)
+            self._q = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def trajectory_batch(fields, particles, ctstart, ctstop, t0, npoints):
+    """RK4 trajectories of particles with per-particle ctstart/ctstop/t0/npoints (sequences) in one
+    launch (srs_trajectory_batch).  Returns one device.Trajectory (nparticles = 1) per particle, all
+    views into one allocation."""
+    import torch
+    P = len(particles)
+    ctstart, ctstop, t0 = (np.broadcast_to(np.asarray(v, float), (P,)).copy() for v in (ctstart, ctstop, t0))
+    npoints = np.broadcast_to(np.asarray(npoints, np.int64), (P,)).copy()
+    shapes = [device.counts(ctstart[p], ctstop[p], t0[p], int(npoints[p])) for p in range(P)]
+    sizes = [3 * (nf + nb) for _, nf, nb in shapes]
+    total = int(sum(sizes))
+    buf = torch.empty((3, total), dtype=torch.float64, device="cuda")
+    trajs, off = [], 0
+    for (dt, nf, nb), s in zip(shapes, sizes):
+        v = [buf[k, off:off + s].view(1, 3, nf + nb) for k in range(3)]
+        trajs.append(device.Trajectory(v[0], v[1], v[2], dt))
+        off += s
+    fa = (_lib.Field * max(1, len(fields)))(*fields)
+    pa = (_lib.Particle * P)(*particles)
+    ptrs = [(C.c_void_p * P)(*[getattr(t, a).data_ptr() for t in trajs]) for a in ("x", "beta", "aoc")]
+    D = _lib._D
+    check(lib.srs_trajectory_batch(fa, len(fields), pa, P, ctstart.ctypes.data_as(D), ctstop.ctypes.data_as(D),
+                                   t0.ctypes.data_as(D), npoints.ctypes.data_as(C.POINTER(C.c_int64)),
+                                   ptrs[0], ptrs[1], ptrs[2], device._stream()))
+    return trajs
+
+
+def signature(jobs):
+    """Shape signature of a job list (kinds, trajectory lengths, output sizes) and the device."""
+    import torch
+    h = hashlib.sha1()
+    for j, _ in jobs:
+        out = j.grid.n1 * j.grid.n2 if j.kind == _lib.JOB_FLUX else j.ne
+        h.update(f"{j.kind}:{j.traj.n}:{out};".encode())
+    h.update(torch.cuda.get_device_name().encode())
+    return h.hexdigest()[:20]
+
+
+def _cache_path():
+    return os.environ.get("SRS_B200_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "srsoriginal_b200", "queue_tune.json"))
+
+
+def time_queue(q, reps=5, warmup=2):
+    """Mean device time [ms] of q.run() over reps runs (CUDA events on the current stream)."""
+    import torch
+    for _ in range(warmup):
+        q.run()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    for _ in range(reps):
+        q.run()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def autotune(jobs, chunks=CHUNKS, ctas_per_sm=CTAS_PER_SM, reps=3, cache=True):
+    """Pick (chunk, ctas_per_sm) for this job list by timing every candidate queue on the jobs
+    themselves.  Returns (chunk, ctas_per_sm, table) with table = {(chunk, ctas): ms}.  With cache, a
+    previous result for the same signature is returned without timing, and new results are stored."""
+    key = signature(jobs)
+    path = _cache_path()
+    db = {}
+    if cache and os.path.exists(path):
+        try:
+            with open(path) as f:
+                db = json.load(f)
+        except (OSError, ValueError):
+            db = {}
+        if key in db:
+            r = db[key]
+            return int(r["chunk"]), int(r["ctas_per_sm"]), {}
+    table = {}
+    for ch in chunks:
+        for c in ctas_per_sm:
+            q = JobQueue(jobs, ch, c)
+            table[(ch, c)] = time_queue(q, reps)
+            q.close()
+    (ch, c), ms = min(table.items(), key=lambda kv: kv[1])
+    if cache:
+        db[key] = {"chunk": ch, "ctas_per_sm": c, "ms": ms}
+        try:
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            with open(path, "w") as f:
+                json.dump(db, f, indent=1)
+        except OSError:
+            pass
+    return ch, c, table

@@ -103,3 +103,39 @@ def config3b_jobs(n=256, seed=3):
         else:
             jobs.append(dict(kind="flux", nt=nt, n=int(rng.integers(8, 202))))
     return jobs
+
+
+def build_config3b(specs, chunk=None, ctas_per_sm=0, tune=False):
+    """Device jobs of a config-3b style spec list (from :func:`config3b_jobs`): the ideal 3 GeV
+    particle through the config-0 undulator, each job with its own trajectory length (all computed
+    by one srs_trajectory_batch launch), flux maps on a 10 mm square at 30 m at E1, spectra on axis
+    at 30 m over the reference's 100-1000 eV energy grid.  Returns (JobQueue, jobs, trajectories);
+    job outputs are jobs[i][1][-1].  tune: pick (chunk, CTAs per SM) with queue.autotune."""
+    import torch
+
+    from . import device as D
+    from . import queue as Q
+    from .sr import energy_grid, rectangle_points
+
+    und = D.undulator([0, BPEAK, 0], [0, 0, PERIOD], NPERIODS)
+    part, _ = D.ideal_particle(ENERGY_GEV, [0, 0, -1], [0, 0, 1])
+    trajs = Q.trajectory_batch([und], [part] * len(specs), 0.0, 2.0, 0.0, [s["nt"] for s in specs])
+    charge, current = -D.QE, CURRENT
+    jobs, grids, energies = [], {}, {}
+    for s, t in zip(specs, trajs):
+        if s["kind"] == "flux":
+            n = s["n"]
+            if n not in grids:
+                grids[n] = rectangle_points([n, n], plane="XY", width=[0.01, 0.01], translation=[0, 0, SCREEN_Z])[3]
+            out = torch.empty(n * n, dtype=torch.float64, device="cuda")
+            jobs.append(Q.flux_job(t, charge, current, grids[n], E1_EV, out))
+        else:
+            ne = s["ne"]
+            if ne not in energies:
+                energies[ne] = torch.tensor(energy_grid(ne, 100.0, 1000.0), dtype=torch.float64, device="cuda")
+            out = torch.empty(ne, dtype=torch.float64, device="cuda")
+            jobs.append(Q.spectrum_job(t, charge, current, [0, 0, SCREEN_Z], energies[ne], out))
+    if tune:
+        chunk, ctas_per_sm, _ = Q.autotune(jobs)
+    q = Q.JobQueue(jobs, chunk or 2048, ctas_per_sm)
+    return q, jobs, trajs
