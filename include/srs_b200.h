@@ -188,6 +188,39 @@ srs_status srs_total_power(srs_traj_view traj, srs_beam_consts beam, const doubl
 srs_status srs_accumulate(const double *d_vals, int32_t nparticles, int64_t nout, double weight,
                           double *out, double *comp, void *stream);
 
+/* ------------------------------------------------------------------ derivatives
+ * No counterpart in the reference (it has no derivatives): the hand-written adjoint of
+ * flux_k = C2 (C0 w_k dt)^2 |E_k|^2 on a spectrum (OSCARSSR.cc:1154-1251) back through the RK4
+ * trajectory (OSCARSSR.cc:562-874) to the field parameters and the initial conditions. */
+
+/* srs_spectrum that also returns the sums E_k: d_e6 (DEVICE, nparticles*ne*6) receives Re/Im of
+ * E_x, E_y, E_z of every output, before the final scaling.  d_flux as srs_spectrum's d_out. */
+srs_status srs_spectrum_efield(srs_traj_view traj, srs_beam_consts beam, const double obs[3],
+                               const double *d_energies, int64_t ne, int32_t precision, double *d_flux,
+                               double *d_e6, void *stream);
+
+/* Adjoint of the spectrum sum for one particle: given E_k (d_e6, from srs_spectrum_efield) and
+ * d_gflux = dL/dflux_k (DEVICE, ne), writes dL/dx_i and dL/dbeta_i of every trajectory point to d_gx,
+ * d_gbeta (DEVICE, 3*n each, layout as the trajectory).  FP64. */
+srs_status srs_spectrum_adjoint(srs_traj_view traj, srs_beam_consts beam, const double obs[3],
+                                const double *d_energies, int64_t ne, const double *d_e6,
+                                const double *d_gflux, double *d_gx, double *d_gbeta, void *stream);
+
+/* Adjoint of the RK4 trajectory of one particle (the same arguments as srs_trajectory, with the
+ * trajectory it wrote in d_x, d_beta): given dL/dx_i, dL/dbeta_i (d_gx, d_gbeta), accumulates
+ *   grid_grads[f] (HOST array of nfields DEVICE pointers, entries may be NULL; for grid fields:
+ *       3*nsamples values, dL/d(sample), ADDED to what is there),
+ *   amp_grad (HOST, 3*nfields, may be NULL; dL/d(field vector) of undulator, Gaussian and uniform
+ *       fields, 0 for grids),
+ *   ic_grad (HOST, 7): dL/dx0[3], dL/dbeta0[3], dL/d(q/(m gamma)).
+ * At most 16 fields.  The recurrence lambda_j = g_j + J_j^T lambda_{j+1} is solved as a parallel
+ * scan over the stored states (no serial sweep).  Synchronises the stream (host outputs). */
+srs_status srs_trajectory_adjoint(const srs_field *fields, int32_t nfields, const srs_particle *particle,
+                                  double ctstart, double ctstop, double t0, int64_t npoints,
+                                  const double *d_x, const double *d_beta, const double *d_gx,
+                                  const double *d_gbeta, double *const *grid_grads, double *amp_grad,
+                                  double *ic_grad, void *stream);
+
 /* ------------------------------------------------------------------ heterogeneous work queue
  * No counterpart in the reference (which runs one calculation per call, each with its own launch
  * and host synchronisation, OSCARSSR.cc:1154-1251 and 1989-2099): a set of mixed-precision flux and

@@ -28,6 +28,7 @@ SOURCES = [
     ("sums_fp64.cu", True),
     ("sums_mixed.cu", False),
     ("queue.cu", False),
+    ("adjoint.cu", True),
     ("capi.cu", True),
     ("sim.cpp", True),
     ("peaks.cu", False),

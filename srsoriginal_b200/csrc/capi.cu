@@ -88,7 +88,8 @@ srs_status srs_trajectory(const srs_field *fields, int32_t nfields, const srs_pa
   SRS_CUDA(dp.alloc(sizeof(srs_particle) * nparticles, s));
   if (nfields > 0) SRS_CUDA(cudaMemcpyAsync(df.ptr, fields, sizeof(srs_field) * nfields, cudaMemcpyHostToDevice, s));
   SRS_CUDA(cudaMemcpyAsync(dp.ptr, particles, sizeof(srs_particle) * nparticles, cudaMemcpyHostToDevice, s));
-  SRS_CUDA(launch_rk4(df.as<srs_field>(), nfields, dp.as<srs_particle>(), nparticles, dt, nf, nb, d_x, d_beta, d_aoc, s));
+  SRS_CUDA(launch_rk4(df.as<srs_field>(), nfields, dp.as<srs_particle>(), nparticles, dt, nf, nb, d_x, d_beta, d_aoc, s,
+                      nfields > 0 ? grid_stage_doubles(fields, nfields) : 0));
   return SRS_OK;
 }
 

@@ -32,6 +32,8 @@ namespace srs {
 namespace {
 
 constexpr int kMaxFieldsShared = 16;
+// grid samples staged in shared memory when all grid fields together fit (192 KB)
+constexpr int64_t kGridStageMaxDoubles = 24576;
 
 // a / b rounded to nearest, given rb = RN(1/b): one multiply and Markstein's FMA correction step
 // (P. Markstein, IBM J. Res. Dev. 34(1), 1990): with q = RN(a rb) faithful and r = a - b q exact,
@@ -48,10 +50,12 @@ struct Prepared {
   double F[3], C[3], u[3];
   double plen, rplen, ps, taper, b_lo, b_hi, e1_lo, e1_hi, e2_lo, e2_hi;  // undulator
   double rs[3], rc[3];                                                     // rotation sines / cosines
+  const double *gd;                                                        // grid samples (shared or global)
 };
 
 __device__ void prepare(const srs_field &f, Prepared &p) {
   p.kind = f.kind;
+  p.gd = f.data;
   for (int c = 0; c < 3; ++c) {
     p.F[c] = f.field[c];
     p.C[c] = f.center[c];
@@ -118,8 +122,8 @@ __device__ inline V3 field_one(const Prepared &p, const srs_field &f, V3 X) {
         return v3(0, 0, 0);
       return ld3(p.F);
     }
-    case SRS_FIELD_GRID:
-      return grid_field(f, X);
+    case SRS_FIELD_GRID:  // grid_field with the rotation's sines and cosines precomputed
+      return grid_interp(f, p.gd, rotate_pre(X, p) - ld3(f.translation));
     default:
       return v3(0, 0, 0);
   }
@@ -131,6 +135,30 @@ __device__ inline V3 force(double qomg, V3 v, V3 B) {
 }
 
 __device__ inline V3 vadd_scaled(V3 a, double h, V3 b) { return v3(a.x + h * b.x, a.y + h * b.y, a.z + h * b.z); }
+
+// Copies every grid field's samples into the block's dynamic shared memory (the launcher sizes it to
+// the total when that fits) and points the prepared fields at the copies: the interpolation then
+// reads shared memory instead of global memory inside the serial RK4 chain.
+extern __shared__ double g_stage[];
+__device__ void stage_grids(const srs_field *sf, Prepared *sp, int nfields) {
+  int64_t off = 0;
+  for (int i = 0; i < nfields; ++i) {
+    if (sf[i].kind != SRS_FIELD_GRID) continue;
+    const int64_t cnt = 3 * sf[i].n[0] * sf[i].n[1] * sf[i].n[2];
+    for (int64_t k = threadIdx.x; k < cnt; k += blockDim.x) g_stage[off + k] = sf[i].data[k];
+    off += cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    off = 0;
+    for (int i = 0; i < nfields; ++i) {
+      if (sf[i].kind != SRS_FIELD_GRID) continue;
+      sp[i].gd = g_stage + off;
+      off += 3 * sf[i].n[0] * sf[i].n[1] * sf[i].n[2];
+    }
+  }
+  __syncthreads();
+}
 
 // ---------------------------------------------------------------- warp-cooperative kernel
 
@@ -145,7 +173,8 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
                                                        const srs_particle *__restrict__ particles, int nparticles,
                                                        double dt_all, int64_t nfwd_all, int64_t nbwd_all, int G,
                                                        double *__restrict__ X, double *__restrict__ Bt,
-                                                       double *__restrict__ A, const TrajSpec *__restrict__ specs) {
+                                                       double *__restrict__ A, const TrajSpec *__restrict__ specs,
+                                                       int64_t stage_doubles) {
   __shared__ srs_field sf[kMaxFieldsShared];
   __shared__ Prepared sp[kMaxFieldsShared];
   for (int i = threadIdx.x; i < nfields; i += blockDim.x) {
@@ -153,6 +182,7 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
     prepare(sf[i], sp[i]);
   }
   __syncthreads();
+  if (stage_doubles > 0) stage_grids(sf, sp, nfields);
   const int lane = threadIdx.x & 31;
   const int gl = lane & (G - 1), gbase = lane - gl;
   const int pp = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 / G) + lane / G;
@@ -250,7 +280,7 @@ __global__ void __launch_bounds__(64) rk4_thread_kernel(const srs_field *__restr
                                                         const srs_particle *__restrict__ particles, int nparticles,
                                                         double dt, int64_t nfwd, int64_t nbwd,
                                                         double *__restrict__ X, double *__restrict__ Bt,
-                                                        double *__restrict__ A) {
+                                                        double *__restrict__ A, int64_t stage_doubles) {
   __shared__ srs_field sf[kMaxFieldsShared];
   __shared__ Prepared sp[kMaxFieldsShared];
   for (int i = threadIdx.x; i < nfields; i += blockDim.x) {
@@ -258,6 +288,7 @@ __global__ void __launch_bounds__(64) rk4_thread_kernel(const srs_field *__restr
     prepare(sf[i], sp[i]);
   }
   __syncthreads();
+  if (stage_doubles > 0) stage_grids(sf, sp, nfields);
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nparticles) return;
   const srs_particle P = particles[p];
@@ -334,36 +365,58 @@ static int group_size(int nparticles, int nfields) {
   return G;
 }
 
+int64_t grid_stage_doubles(const srs_field *host_fields, int nfields) {
+  int64_t total = 0;
+  for (int i = 0; i < nfields; ++i)
+    if (host_fields[i].kind == SRS_FIELD_GRID)
+      total += 3 * host_fields[i].n[0] * host_fields[i].n[1] * host_fields[i].n[2];
+  return total <= kGridStageMaxDoubles ? total : 0;
+}
+
+namespace {
+// The 48 KB default covers static plus dynamic shared memory; raise the kernel's dynamic limit
+// whenever grid samples are staged.
+template <typename K>
+cudaError_t allow_smem(K kernel, size_t bytes) {
+  if (bytes == 0) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+}  // namespace
+
 cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
                        double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
-                       cudaStream_t s) {
+                       cudaStream_t s, int64_t stage_doubles) {
   if (nparticles <= 0) return cudaSuccess;
   if (nfields > kMaxFieldsShared) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(double) * (size_t)stage_doubles;
   const int G = group_size(nparticles, nfields);
   // grouped lanes while there are few particles per SM (the serial chain is the limit); one thread
   // per particle when there are enough particles to fill the SMs (issue rate is the limit)
   if (G <= 32 && (int64_t)nparticles * G <= 148 * 32 * 48) {
     const int warps = 4, per_block = warps * (32 / G);
-    rk4_warp_kernel<<<(nparticles + per_block - 1) / per_block, 32 * warps, 0, s>>>(
-        d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, G, d_x, d_b, d_a, nullptr);
+    if (cudaError_t e = allow_smem(rk4_warp_kernel, smem)) return e;
+    rk4_warp_kernel<<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
+        d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, G, d_x, d_b, d_a, nullptr, stage_doubles);
   } else {
     const int threads = 64;
-    rk4_thread_kernel<<<(nparticles + threads - 1) / threads, threads, 0, s>>>(d_fields, nfields, d_particles,
-                                                                               nparticles, dt, nfwd, nbwd, d_x, d_b,
-                                                                               d_a);
+    if (cudaError_t e = allow_smem(rk4_thread_kernel, smem)) return e;
+    rk4_thread_kernel<<<(nparticles + threads - 1) / threads, threads, smem, s>>>(
+        d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, stage_doubles);
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_rk4_specs(const srs_field *d_fields, int nfields, const srs_particle *d_particles,
-                             const TrajSpec *d_specs, int nparticles, cudaStream_t s) {
+                             const TrajSpec *d_specs, int nparticles, cudaStream_t s, int64_t stage_doubles) {
   if (nparticles <= 0) return cudaSuccess;
   if (nfields > kMaxFieldsShared) return cudaErrorInvalidValue;
   const int G = group_size(nparticles, nfields);
   if (G > 32) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(double) * (size_t)stage_doubles;
+  if (cudaError_t e = allow_smem(rk4_warp_kernel, smem)) return e;
   const int warps = 4, per_block = warps * (32 / G);
-  rk4_warp_kernel<<<(nparticles + per_block - 1) / per_block, 32 * warps, 0, s>>>(
-      d_fields, nfields, d_particles, nparticles, 0.0, 0, 0, G, nullptr, nullptr, nullptr, d_specs);
+  rk4_warp_kernel<<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
+      d_fields, nfields, d_particles, nparticles, 0.0, 0, 0, G, nullptr, nullptr, nullptr, d_specs, stage_doubles);
   return cudaGetLastError();
 }
 

@@ -335,7 +335,8 @@ struct srs_sim {
     SRS_CUDA(dp.alloc(sizeof(srs_particle) * np, stream));
     SRS_CUDA(cudaMemcpyAsync(dp.ptr, hp.data(), sizeof(srs_particle) * np, cudaMemcpyHostToDevice, stream));
     SRS_CUDA(launch_rk4(reinterpret_cast<const srs_field *>(d_fields), (int)fields.size(), dp.as<srs_particle>(), np,
-                        dt, nf, nb, X, B, A, stream));
+                        dt, nf, nb, X, B, A, stream,
+                        fields.empty() ? 0 : grid_stage_doubles(fields.data(), (int)fields.size())));
     view.x = X;
     view.beta = B;
     view.aoc = A;

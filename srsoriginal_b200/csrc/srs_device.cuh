@@ -121,16 +121,13 @@ __device__ inline V3 box_field(const srs_field &f, V3 X) {
   return ld3(f.field);
 }
 
-// TField3D_Grid::GetF (src/TField3D_Grid.cc:124-243): rotate, translate, zero outside, then linear /
-// bilinear / trilinear interpolation in x -> y -> z order with the reference's arithmetic.
-__device__ inline V3 grid_at(const srs_field &f, int64_t ix, int64_t iy, int64_t iz) {
-  return ld3(f.data + 3 * (ix * f.n[1] * f.n[2] + iy * f.n[2] + iz));
+__device__ inline V3 grid_at(const double *data, const srs_field &f, int64_t ix, int64_t iy, int64_t iz) {
+  return ld3(data + 3 * (ix * f.n[1] * f.n[2] + iy * f.n[2] + iz));
 }
 __device__ inline V3 grid_lerp(V3 a, V3 b, double d, double step) { return a + (b - a) * d / step; }
-__device__ inline V3 grid_field(const srs_field &f, V3 XIN) {
-  V3 X = XIN;
-  rotate_xyz(X, f.rotations);
-  X = X - ld3(f.translation);
+// Interpolation at X, already in the grid's frame (rotated and translated); samples read from data
+// (the field's own array, or a copy of it in shared memory).
+__device__ inline V3 grid_interp(const srs_field &f, const double *data, V3 X) {
   const bool hx = f.n[0] > 1, hy = f.n[1] > 1, hz = f.n[2] > 1;
   if (hx && (X.x <= f.start[0] || X.x >= f.start[0] + (double)(f.n[0] - 1) * f.step[0])) return v3(0, 0, 0);
   if (hy && (X.y <= f.start[1] || X.y >= f.start[1] + (double)(f.n[1] - 1) * f.step[1])) return v3(0, 0, 0);
@@ -146,34 +143,44 @@ __device__ inline V3 grid_field(const srs_field &f, V3 XIN) {
   if (hx && nx > (uint64_t)(f.n[0] - 2)) nx = f.n[0] - 2;
   if (hy && ny > (uint64_t)(f.n[1] - 2)) ny = f.n[1] - 2;
   if (hz && nz > (uint64_t)(f.n[2] - 2)) nz = f.n[2] - 2;
+  const double *d = data;
   if (hx && hy && hz) {
-    V3 v00 = grid_lerp(grid_at(f, nx, ny, nz), grid_at(f, nx + 1, ny, nz), dx, f.step[0]);
-    V3 v10 = grid_lerp(grid_at(f, nx, ny + 1, nz), grid_at(f, nx + 1, ny + 1, nz), dx, f.step[0]);
-    V3 v01 = grid_lerp(grid_at(f, nx, ny, nz + 1), grid_at(f, nx + 1, ny, nz + 1), dx, f.step[0]);
-    V3 v11 = grid_lerp(grid_at(f, nx, ny + 1, nz + 1), grid_at(f, nx + 1, ny + 1, nz + 1), dx, f.step[0]);
+    V3 v00 = grid_lerp(grid_at(d, f, nx, ny, nz), grid_at(d, f, nx + 1, ny, nz), dx, f.step[0]);
+    V3 v10 = grid_lerp(grid_at(d, f, nx, ny + 1, nz), grid_at(d, f, nx + 1, ny + 1, nz), dx, f.step[0]);
+    V3 v01 = grid_lerp(grid_at(d, f, nx, ny, nz + 1), grid_at(d, f, nx + 1, ny, nz + 1), dx, f.step[0]);
+    V3 v11 = grid_lerp(grid_at(d, f, nx, ny + 1, nz + 1), grid_at(d, f, nx + 1, ny + 1, nz + 1), dx, f.step[0]);
     V3 v0 = grid_lerp(v00, v10, dy, f.step[1]);
     V3 v1 = grid_lerp(v01, v11, dy, f.step[1]);
     return grid_lerp(v0, v1, dz, f.step[2]);
   } else if (hx && hy) {
-    V3 v0 = grid_lerp(grid_at(f, nx, ny, 0), grid_at(f, nx + 1, ny, 0), dx, f.step[0]);
-    V3 v1 = grid_lerp(grid_at(f, nx, ny + 1, 0), grid_at(f, nx + 1, ny + 1, 0), dx, f.step[0]);
+    V3 v0 = grid_lerp(grid_at(d, f, nx, ny, 0), grid_at(d, f, nx + 1, ny, 0), dx, f.step[0]);
+    V3 v1 = grid_lerp(grid_at(d, f, nx, ny + 1, 0), grid_at(d, f, nx + 1, ny + 1, 0), dx, f.step[0]);
     return grid_lerp(v0, v1, dy, f.step[1]);
   } else if (hx && hz) {
-    V3 v0 = grid_lerp(grid_at(f, nx, 0, nz), grid_at(f, nx + 1, 0, nz), dx, f.step[0]);
-    V3 v1 = grid_lerp(grid_at(f, nx, 0, nz + 1), grid_at(f, nx + 1, 0, nz + 1), dx, f.step[0]);
+    V3 v0 = grid_lerp(grid_at(d, f, nx, 0, nz), grid_at(d, f, nx + 1, 0, nz), dx, f.step[0]);
+    V3 v1 = grid_lerp(grid_at(d, f, nx, 0, nz + 1), grid_at(d, f, nx + 1, 0, nz + 1), dx, f.step[0]);
     return grid_lerp(v0, v1, dz, f.step[2]);
   } else if (hy && hz) {
-    V3 v0 = grid_lerp(grid_at(f, 0, ny, nz), grid_at(f, 0, ny + 1, nz), dy, f.step[1]);
-    V3 v1 = grid_lerp(grid_at(f, 0, ny, nz + 1), grid_at(f, 0, ny + 1, nz + 1), dy, f.step[1]);
+    V3 v0 = grid_lerp(grid_at(d, f, 0, ny, nz), grid_at(d, f, 0, ny + 1, nz), dy, f.step[1]);
+    V3 v1 = grid_lerp(grid_at(d, f, 0, ny, nz + 1), grid_at(d, f, 0, ny + 1, nz + 1), dy, f.step[1]);
     return grid_lerp(v0, v1, dz, f.step[2]);
   } else if (hx) {
-    return grid_lerp(ld3(f.data + 3 * nx), ld3(f.data + 3 * (nx + 1)), dx, f.step[0]);
+    return grid_lerp(ld3(d + 3 * nx), ld3(d + 3 * (nx + 1)), dx, f.step[0]);
   } else if (hy) {
-    return grid_lerp(ld3(f.data + 3 * ny), ld3(f.data + 3 * (ny + 1)), dy, f.step[1]);
+    return grid_lerp(ld3(d + 3 * ny), ld3(d + 3 * (ny + 1)), dy, f.step[1]);
   } else if (hz) {
-    return grid_lerp(ld3(f.data + 3 * nz), ld3(f.data + 3 * (nz + 1)), dz, f.step[2]);
+    return grid_lerp(ld3(d + 3 * nz), ld3(d + 3 * (nz + 1)), dz, f.step[2]);
   }
   return v3(0, 0, 0);
+}
+
+// TField3D_Grid::GetF (src/TField3D_Grid.cc:124-243): rotate, translate, zero outside, then linear /
+// bilinear / trilinear interpolation in x -> y -> z order with the reference's arithmetic.
+__device__ inline V3 grid_field(const srs_field &f, V3 XIN) {
+  V3 X = XIN;
+  rotate_xyz(X, f.rotations);
+  X = X - ld3(f.translation);
+  return grid_interp(f, f.data, X);
 }
 
 // TFieldContainer::GetF (src/TFieldContainer.cc:92-103): Sum(0,0,0) += each field.

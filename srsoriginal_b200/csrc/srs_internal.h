@@ -54,18 +54,23 @@ struct TrajSpec {
 };
 
 // ---- kernel launchers ----
+// Grid samples (doubles) to stage in shared memory for these fields (HOST array): their total, or 0
+// when they do not fit.  Pass it to the RK4 launchers.
+int64_t grid_stage_doubles(const srs_field *host_fields, int nfields);
 cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
                        double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
-                       cudaStream_t s);
+                       cudaStream_t s, int64_t stage_doubles);
 cudaError_t launch_rk4_specs(const srs_field *d_fields, int nfields, const srs_particle *d_particles,
-                             const TrajSpec *d_specs, int nparticles, cudaStream_t s);
+                             const TrajSpec *d_specs, int nparticles, cudaStream_t s, int64_t stage_doubles);
 cudaError_t launch_field_eval(const srs_field *d_fields, int nfields, const double *d_xyz, int64_t np,
                               double *d_out, cudaStream_t s);
 
 // Plain FP64 sums.  Scratch is caller-provided (size from the *_scratch_bytes functions).
 size_t fp64_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles);
+// d_e6 (optional): the reduced sums SumE (Re/Im of x, y, z) of every output, 6 per output.
 cudaError_t fp64_spectrum(const srs_traj_view &t, const srs_beam_consts &b, const double obs[3],
-                          const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s);
+                          const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s,
+                          double *d_e6 = nullptr);
 size_t fp64_flux_scratch_bytes(int64_t n, int64_t np, int nparticles);
 cudaError_t fp64_flux(const srs_traj_view &t, const srs_beam_consts &b, const double *d_points, int64_t np,
                       double energy_ev, double *d_out, void *scratch, cudaStream_t s);
@@ -81,7 +86,8 @@ cudaError_t accumulate_particles(const double *d_vals, int nparticles, int64_t n
 // Mixed-precision sums.
 size_t mixed_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles);
 cudaError_t mixed_spectrum(const srs_traj_view &t, const srs_beam_consts &b, const double obs[3],
-                           const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s);
+                           const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s,
+                           double *d_e6 = nullptr);
 size_t mixed_flux_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles);
 cudaError_t mixed_flux(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g, double energy_ev,
                        double *d_out, void *scratch, cudaStream_t s);
@@ -92,7 +98,8 @@ cudaError_t mixed_power_density(const srs_traj_view &t, const srs_beam_consts &b
 // Finishing kernels shared by both precisions: add the S per-chunk partial sums in chunk order and
 // apply the reference's final scaling.
 cudaError_t finish_flux_partials(const double *partial, int S, int64_t nout, int nparticles, const double *omegas,
-                                 double omega0, double dt, double C0, double C2, double *out, cudaStream_t s);
+                                 double omega0, double dt, double C0, double C2, double *out, cudaStream_t s,
+                                 double *e6 = nullptr);
 cudaError_t finish_pd_partials(const double *partial, int S, int64_t np, int nparticles, double cdt, int directional,
                                double *out, cudaStream_t s);
 

@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kTile) flux_fp64_kernel(const double *__restri
 
 __global__ void flux_fp64_reduce(const double *__restrict__ partial, int S, int64_t np, int nparticles,
                                  const double *__restrict__ omegas, double omega0, double dt, double C0, double C2,
-                                 double *__restrict__ out) {
+                                 double *__restrict__ out, double *__restrict__ e6) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= np * nparticles) return;
   const int64_t p = idx / np, j = idx % np;
@@ -103,6 +103,10 @@ __global__ void flux_fp64_reduce(const double *__restrict__ partial, int S, int6
   }
   const double omega = omegas ? omegas[j] : omega0;
   out[idx] = finish_flux(e, omega, dt, C0, C2);
+  if (e6) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) e6[6 * idx + c] = e[c];
+  }
 }
 
 // ---------------------------------------------------------------- spectrum at one observer
@@ -287,7 +291,7 @@ cudaError_t fp64_flux(const srs_traj_view &t, const srs_beam_consts &b, const do
   flux_fp64_kernel<<<grid, kTile, 0, s>>>(t.x, t.beta, t.n, t.dt, d_points, np, omega, chunk, partial);
   flux_fp64_reduce<<<blocks_for(np * t.nparticles, 256), 256, 0, s>>>(partial, S, np, t.nparticles, nullptr, omega,
                                                                       t.dt, flux_c0(b.charge),
-                                                                      flux_c2(b.charge, b.current), d_out);
+                                                                      flux_c2(b.charge, b.current), d_out, nullptr);
   return cudaGetLastError();
 }
 
@@ -296,7 +300,8 @@ size_t fp64_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles) {
 }
 
 cudaError_t fp64_spectrum(const srs_traj_view &t, const srs_beam_consts &b, const double obs[3],
-                          const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s) {
+                          const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s,
+                          double *d_e6) {
   if (ne <= 0 || t.nparticles <= 0) return cudaSuccess;
   const int S = flux_splits(t.n, ne, t.nparticles);
   const int64_t chunk = (t.n + S - 1) / S;
@@ -308,7 +313,7 @@ cudaError_t fp64_spectrum(const srs_traj_view &t, const srs_beam_consts &b, cons
   omegas_kernel<<<blocks_for(ne, 256), 256, 0, s>>>(d_energies, ne, omegas);
   flux_fp64_reduce<<<blocks_for(ne * t.nparticles, 256), 256, 0, s>>>(partial, S, ne, t.nparticles, omegas, 0.0,
                                                                       t.dt, flux_c0(b.charge),
-                                                                      flux_c2(b.charge, b.current), d_out);
+                                                                      flux_c2(b.charge, b.current), d_out, d_e6);
   return cudaGetLastError();
 }
 
@@ -341,9 +346,10 @@ cudaError_t total_power(const srs_traj_view &t, const srs_beam_consts &b, const 
 }
 
 cudaError_t finish_flux_partials(const double *partial, int S, int64_t nout, int nparticles, const double *omegas,
-                                 double omega0, double dt, double C0, double C2, double *out, cudaStream_t s) {
+                                 double omega0, double dt, double C0, double C2, double *out, cudaStream_t s,
+                                 double *e6) {
   flux_fp64_reduce<<<blocks_for(nout * nparticles, 256), 256, 0, s>>>(partial, S, nout, nparticles, omegas, omega0, dt,
-                                                                     C0, C2, out);
+                                                                     C0, C2, out, e6);
   return cudaGetLastError();
 }
 

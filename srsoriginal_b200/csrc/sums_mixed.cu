@@ -290,7 +290,8 @@ size_t mixed_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles) {
 }
 
 cudaError_t mixed_spectrum(const srs_traj_view &t, const srs_beam_consts &b, const double obs[3],
-                           const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s) {
+                           const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s,
+                           double *d_e6) {
   const int64_t etiles = (ne + kThreads * kEnergiesPerThread - 1) / (kThreads * kEnergiesPerThread);
   const int S = splits_for(etiles * t.nparticles, t.n, 256);
   const int64_t chunk = (t.n + S - 1) / S;
@@ -303,7 +304,7 @@ cudaError_t mixed_spectrum(const srs_traj_view &t, const srs_beam_consts &b, con
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return finish_flux_partials(partial, S, ne, t.nparticles, omegas, 0.0, t.dt, flux_c0(b.charge),
-                              flux_c2(b.charge, b.current), d_out, s);
+                              flux_c2(b.charge, b.current), d_out, s, d_e6);
 }
 
 }  // namespace srs

@@ -139,3 +139,57 @@ def build_config3b(specs, chunk=None, ctas_per_sm=0, tune=False):
         chunk, ctas_per_sm, _ = Q.autotune(jobs)
     q = Q.JobQueue(jobs, chunk or 2048, ctas_per_sm)
     return q, jobs, trajs
+
+
+NE4 = 200  # config 4: energies over +-2 % of E3 (reference energy grid)
+IC_NAMES = ("x", "y", "x'", "y'", "z", "E")
+IC4 = (0.0, 0.0, 0.0, 0.0, -1.0, ENERGY_GEV)
+# coordinate scales for the finite-difference steps h = 1e-6 * max(|value|, scale): field samples [T],
+# then x, y [m], x', y' [rad], z [m], E [GeV]
+FD_SCALES = (1.0, 1e-3, 1e-3, 1e-3, 1e-3, 1.0, 1.0)
+
+
+def config4_energy_range():
+    return 0.98 * E3_EV, 1.02 * E3_EV
+
+
+def config4_coords(n=32, seed=4, nsamples=2001):
+    """The coordinates checked by finite differences, as indices into (grid samples By_0 ..
+    By_{nsamples-1}, then x, y, x', y', z, E): n distinct indices drawn with numpy default_rng(seed),
+    then the six initial-condition coordinates (which a random draw of 32 from 2007 rarely hits)."""
+    drawn = np.random.default_rng(seed).choice(nsamples + 6, size=n, replace=False)
+    extra = [k for k in range(nsamples, nsamples + 6) if k not in set(drawn.tolist())]
+    return np.concatenate([drawn, np.array(extra, dtype=drawn.dtype)])
+
+
+def config4_fd_step(k, by, ic=IC4, rel=1e-6):
+    nz = len(by)
+    if k < nz:
+        return rel * max(abs(float(by[k])), FD_SCALES[0])
+    j = k - nz
+    return rel * max(abs(float(ic[j])), FD_SCALES[1 + j])
+
+
+def config4_problem(precision=None, npoints=20001):
+    """(problem, grid, ic, dE) of config 4: the perturbed-undulator 1-D grid (config4_grid) as the
+    only field, the ideal 3 GeV particle from z = -1 m, on-axis flux at 30 m over NE4 energies in
+    +-2 % of E3.  grid: (2001, 3) CUDA tensor (Bx, By, Bz samples); ic: the six coordinates."""
+    import torch
+
+    from . import _lib
+    from . import device as D
+    from .adjoint import SpectrumProblem
+    from .sr import energy_grid
+
+    z, by = config4_grid()
+    dz = float((z[-1] - z[0]) / (len(z) - 1))
+    f = D.grid_z(float(z[0]), dz, by, None)
+    e0, e1 = config4_energy_range()
+    energies = torch.tensor(energy_grid(NE4, e0, e1), dtype=torch.float64, device="cuda")
+    problem = SpectrumProblem(fields=[f], obs=(0.0, 0.0, SCREEN_Z), energies=energies, npoints=npoints,
+                              current=CURRENT, precision=_lib.MIXED if precision is None else precision)
+    g = np.zeros((len(by), 3))
+    g[:, 1] = by
+    grid = torch.tensor(g, dtype=torch.float64, device="cuda")
+    ic = torch.tensor(IC4, dtype=torch.float64)
+    return problem, grid, ic, (e1 - e0) / (NE4 - 1)

@@ -178,6 +178,61 @@ def grid():
          energies=s[:, 0], flux=s[:, 1], bfield=bf)
 
 
+def adjoint():
+    """Config 4 reference gradient: central differences of the reference's own integrated flux
+    -Sum_k flux_k dE through perturbed grid files and beam arguments, on the coordinates the
+    adjoint tests check."""
+    z, by = W.config4_grid()
+    e0, e1 = W.config4_energy_range()
+    de = (e1 - e0) / (W.NE4 - 1)
+
+    def loss(by_, ic):
+        o = new_sr()
+        W.setup_beam(o, 20001, x0=[ic[0], ic[1], ic[4]], d0=[ic[2], ic[3], 1.0], energy_GeV=ic[5])
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "cfg4.txt")
+            W.write_oscars_grid(path, z, by_)
+            o.add_bfield_file(ifile=path, iformat="OSCARS")
+            with redirect_stdout(io.StringIO()):
+                s = o.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], energy_range_eV=[e0, e1], npoints=W.NE4,
+                                         nthreads=NT)
+        f = values(s)
+        return -float(np.sum(f * de)), f
+
+    base, flux = loss(by, list(W.IC4))
+    coords = W.config4_coords()
+    tp, tm, lp, lm = [], [], [], []
+    for k in coords:
+        h = W.config4_fd_step(int(k), by)
+        vals = []
+        for sgn in (+1, -1):
+            b2, ic2 = by.copy(), list(W.IC4)
+            if k < len(by):
+                b2[k] = by[k] + sgn * h
+                t = float(b2[k])
+            else:
+                ic2[k - len(by)] = W.IC4[k - len(by)] + sgn * h
+                t = ic2[k - len(by)]
+            vals.append((t, loss(b2, ic2)[0]))
+        (a, la), (b, lb) = vals
+        tp.append(a); lp.append(la); tm.append(b); lm.append(lb)
+    tp, tm, lp, lm = map(np.array, (tp, tm, lp, lm))
+    # complex-step derivatives of the oracle's analytic restatement of the same forward path, whose
+    # real part must reproduce the reference's loss
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import complex_step as CS
+    from srsoriginal_b200.sr import energy_grid
+    energies = energy_grid(W.NE4, e0, e1)
+    dz = float((z[-1] - z[0]) / (len(z) - 1))
+    g_cs, l_re = CS.complex_step_gradient(by, list(W.IC4), [int(k) for k in coords], float(z[0]), dz,
+                                          [0, 0, W.SCREEN_Z], energies, de)
+    rel = np.abs(l_re - base).max() / abs(base)
+    print("complex-step restatement: loss vs reference", rel)
+    assert rel < 1e-9, rel
+    save("adjoint_cfg4.npz", coords=coords, theta_plus=tp, theta_minus=tm, loss_plus=lp, loss_minus=lm,
+         loss=base, flux=flux, de=de, grad_fd=(lp - lm) / (tp - tm), grad_cs=g_cs, loss_cs=l_re)
+
+
 def quirks():
     """Output-list lengths of the dispatch paths (reference behaviour, kept by the drop-in)."""
     res = {}
@@ -200,7 +255,7 @@ def quirks():
 
 
 if __name__ == "__main__":
-    parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "grid", "quirks"]
+    parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "grid", "adjoint", "quirks"]
     if "cfg0" in parts:
         e1 = cfg0()
         print("E1 (first-harmonic peak of the config-0 spectrum):", repr(e1))
@@ -208,6 +263,7 @@ if __name__ == "__main__":
             print("NOTE: update workloads.E1_EV to", repr(e1))
     if "cfg1" in parts:
         cfg1(W.E1_EV)
-    for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("grid", grid), ("quirks", quirks)):
+    for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("grid", grid), ("adjoint", adjoint),
+                     ("quirks", quirks)):
         if name in parts:
             fn()

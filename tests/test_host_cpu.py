@@ -111,3 +111,28 @@ def test_quirk_fixture_shapes_documented():
     q = json.load(open(os.path.join(ROOT, "tests", "golden", "quirks.json")))
     assert q["flux_len_nthreads1"] == 24 and q["flux_len_nthreads2"] == 12
     assert q["pd_len_nthreads1"] == 12 and q["pd_len_nthreads2"] == 24
+
+
+def test_particle_from_ic_jacobian():
+    """The chain-rule Jacobian d(x0, beta0, q/(m gamma))/d(x, y, x', y', z, E) of the adjoint's
+    initial conditions against central differences (no GPU)."""
+    from srsoriginal_b200.adjoint import particle_from_ic
+
+    def vec(ic):
+        p, _ = particle_from_ic(ic)
+        return np.array(list(p.x0) + list(p.beta0) + [p.qomg])
+
+    ic = np.array([1e-4, -2e-4, 3e-4, -1e-4, -1.0, 3.0])
+    _, J = particle_from_ic(ic)
+    for j in range(6):
+        h = 1e-7 * max(abs(ic[j]), 1e-3)
+        a, b = ic.copy(), ic.copy()
+        a[j] += h
+        b[j] -= h
+        fd = (vec(a) - vec(b)) / (2 * h)
+        scale = np.abs(J).max(axis=1) + 1e-300
+        tol = 1e-6 * scale + 4e-16 * np.abs(vec(ic)) / h  # relative accuracy, plus rounding over 2h
+        # q/(m gamma) takes gamma from |beta0|^2 (as the reference does), 1 - |beta0|^2 ~ 3e-8, so its
+        # rounding is ~1e-16 / 3e-8 relative: the differences carry that noise over 2h
+        tol[6] += 1e-8 * abs(vec(ic)[6]) / h
+        assert np.all(np.abs(fd - J[:, j]) <= tol), (j, fd, J[:, j])
