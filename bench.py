@@ -200,6 +200,131 @@ def run_reference(args, world, rank):
 
 # ------------------------------------------------------------------ our arm
 
+def _events_ms(fn, reps, warmup=1):
+    """Median device time [ms] of fn() over reps runs, CUDA events on the current stream."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    times = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    return statistics.median(times)
+
+
+def measure_configs(dev):
+    """The other configurations' throughput, for the record (not the headline): each device-timed
+    with CUDA events (median of a few runs) unless marked wall-clock."""
+    import numpy as np
+    import torch
+
+    from srsoriginal_b200 import _lib, device as D, queue as Q, workloads as W
+    from srsoriginal_b200.adjoint import backward_flux, forward_flux
+    from srsoriginal_b200.sr import energy_grid, rectangle_points, sr
+
+    out = {}
+    und = [D.undulator([0, W.BPEAK, 0], [0, 0, W.PERIOD], W.NPERIODS)]
+    part, gamma = D.ideal_particle(W.ENERGY_GEV, [0, 0, -1], [0, 0, 1])
+    charge, current = -D.QE, W.CURRENT
+
+    # config 0: plain FP64 on-axis spectrum, 1000 energies (the drop-in path)
+    traj = D.trajectory(und, [part], 0.0, 2.0, 0.0, NT)
+    e0 = torch.tensor(energy_grid(1000, 100.0, 1000.0), dtype=torch.float64, device=dev)
+    sp = torch.empty(1000, dtype=torch.float64, device=dev)
+    ms = _events_ms(lambda: D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sp, precision=_lib.FP64), 5)
+    msm = _events_ms(lambda: D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sp, precision=_lib.MIXED), 5)
+    ev = NT * 1000
+    out["cfg0_spectrum"] = {"evals": ev, "fp64_ms": ms, "fp64_evals_per_s": ev / (ms * 1e-3), "mixed_ms": msm,
+                            "mixed_evals_per_s": ev / (msm * 1e-3)}
+
+    # config 2: power density of the elliptical undulator, 201 x 201 on a 40 mm square, 40001 points
+    epu = [D.undulator([0, 1.0, 0], [0, 0, W.PERIOD], W.NPERIODS),
+           D.undulator([0.6, 0, 0], [0, 0, W.PERIOD], W.NPERIODS, phase=np.pi / 2)]
+    t2 = D.trajectory(epu, [part], 0.0, 2.0, 0.0, 40001)
+    xyz, _, nrm, g2 = rectangle_points([201, 201], "XY", [0.04, 0.04], translation=[0, 0, W.SCREEN_Z])
+    pts = torch.as_tensor(np.ascontiguousarray(xyz.reshape(-1)), device=dev)
+    nrms = torch.as_tensor(np.ascontiguousarray(np.tile(nrm, (201 * 201, 1)).reshape(-1)), device=dev)
+    pd, pd64 = (torch.empty(201 * 201, dtype=torch.float64, device=dev) for _ in range(2))
+    msm = _events_ms(lambda: D.power_density(t2, charge, current, pd, grid=g2, precision=_lib.MIXED), 5)
+    ms = _events_ms(lambda: D.power_density(t2, charge, current, pd64, points=pts, normals=nrms,
+                                            precision=_lib.FP64), 2)
+    a, b = pd.cpu().numpy(), pd64.cpu().numpy()
+    ev = 40001 * 201 * 201
+    out["cfg2_power_density"] = {"evals": ev, "mixed_ms": msm, "mixed_evals_per_s": ev / (msm * 1e-3),
+                                 "fp64_ms": ms, "fp64_evals_per_s": ev / (ms * 1e-3),
+                                 "mixed_over_fp64": ms / msm,
+                                 "mixed_normwise_err_vs_fp64": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
+    del t2, pts, nrms
+
+    # config 3a: 4096 Twiss-sampled electrons, 2000 energies, through the public API (wall clock:
+    # host sampling, 4096 RK4 trajectories, the mixed sums and the per-particle accumulation)
+    o = sr()
+    W.setup_beam(o, NT, **W.BEAM_3A)
+    W.setup_undulator(o)
+    o.set_seed(0)
+    kw = dict(obs=[0, 0, W.SCREEN_Z], npoints=2000, energy_range_eV=[100, 1000], nparticles=4096, precision="mixed")
+    o.spectrum_arrays(**dict(kw, nparticles=64))
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    o.spectrum_arrays(**kw)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t
+    ev = 4096 * NT * 2000
+    out["cfg3a_beam_spectrum"] = {"evals": ev, "wall_s": wall, "evals_per_s": ev / wall,
+                                  "includes": "public API call: sampling, 4096 RK4, mixed sums, accumulation"}
+    del o
+
+    # config 3b: 256 heterogeneous jobs in one persistent launch (CUDA graph), against the same jobs as
+    # separate one-shot calls
+    specs = W.config3b_jobs()
+    q, jobs, trajs = W.build_config3b(specs, chunk=8192, ctas_per_sm=0)
+    ms = _events_ms(q.run, 5)
+
+    def separate():
+        for (j, keep), t_, s_ in zip(jobs, trajs, specs):
+            if s_["kind"] == "flux":
+                D.flux(t_, charge, current, W.E1_EV, keep[-1], grid=j.grid, precision=_lib.MIXED)
+            else:
+                D.spectrum(t_, charge, current, [0, 0, W.SCREEN_Z], keep[1], keep[-1], precision=_lib.MIXED)
+    ms_sep = _events_ms(separate, 3)
+    rk = _events_ms(lambda: Q.trajectory_batch(und, [part] * len(specs), 0.0, 2.0, 0.0, [s_["nt"] for s_ in specs]), 2)
+    out["cfg3b_queue"] = {"evals": q.evals, "queue_ms": ms, "evals_per_s": q.evals / (ms * 1e-3),
+                          "separate_calls_ms": ms_sep, "queue_speedup": ms_sep / ms, "work_items": q.nitems,
+                          "ctas": q.grid, "chunk": q.chunk, "trajectory_batch_ms": rk}
+    q.close()
+    del jobs, trajs
+
+    # config 4: adjoint / forward time (forward = RK4 through the 2001-sample grid + mixed spectrum of
+    # 200 energies; adjoint = sum adjoint + trajectory adjoint scan, FP64)
+    problem, grid, ic, de = W.config4_problem(precision=_lib.MIXED)
+    fw, bw = [], []
+    gfl = None
+    for r in range(6):
+        torch.cuda.synchronize()
+        a_, m_, b_ = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a_.record()
+        f, saved = forward_flux(problem, grid, None, ic, keep_efield=True)
+        m_.record()
+        if gfl is None:
+            gfl = torch.full_like(f, -de)
+        backward_flux(problem, saved, gfl)
+        b_.record()
+        torch.cuda.synchronize()
+        if r > 0:
+            fw.append(a_.elapsed_time(m_))
+            bw.append(m_.elapsed_time(b_))
+    out["cfg4_adjoint"] = {"forward_ms": statistics.median(fw), "adjoint_ms": statistics.median(bw),
+                           "adjoint_over_forward": statistics.median(bw) / statistics.median(fw),
+                           "gradient": "2001 grid samples + 6 initial conditions"}
+    return out
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -337,6 +462,8 @@ def run_ours(args, world, rank, local):
             "rk4_trajectory_ms": rk4_ms,
             "roofline": roofline, "clocks": clk, "e2e": e2e,
             "gpu_launches": args.steps * len(ENERGIES) * 2}
+    if not args.no_configs:
+        line["other_configs"] = measure_configs(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline()
@@ -355,6 +482,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
     args = ap.parse_args()
     if args.impl == "reference":  # host-only: rank 0 runs the reference's CPU path, other ranks exit
         return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))

@@ -35,14 +35,6 @@ constexpr int kMaxFieldsShared = 16;
 // grid samples staged in shared memory when all grid fields together fit (192 KB)
 constexpr int64_t kGridStageMaxDoubles = 24576;
 
-// a / b rounded to nearest, given rb = RN(1/b): one multiply and Markstein's FMA correction step
-// (P. Markstein, IBM J. Res. Dev. 34(1), 1990): with q = RN(a rb) faithful and r = a - b q exact,
-// RN(q + r rb) = RN(a / b) for normal operands without overflow or underflow.
-__device__ __forceinline__ double div_rn(double a, double b, double rb) {
-  const double q = __dmul_rn(a, rb);
-  const double r = __fma_rn(-q, b, a);
-  return __fma_rn(r, rb, q);
-}
 
 // Field constants the reference derives inside GetF (or in Init) from the descriptor.
 struct Prepared {
@@ -51,11 +43,13 @@ struct Prepared {
   double plen, rplen, ps, taper, b_lo, b_hi, e1_lo, e1_hi, e2_lo, e2_hi;  // undulator
   double rs[3], rc[3];                                                     // rotation sines / cosines
   const double *gd;                                                        // grid samples (shared or global)
+  double rstep[3];                                                         // grid: 1 / step per axis
 };
 
 __device__ void prepare(const srs_field &f, Prepared &p) {
   p.kind = f.kind;
   p.gd = f.data;
+  for (int c = 0; c < 3; ++c) p.rstep[c] = f.step[c] != 0 ? 1.0 / f.step[c] : 0.0;
   for (int c = 0; c < 3; ++c) {
     p.F[c] = f.field[c];
     p.C[c] = f.center[c];
@@ -123,7 +117,7 @@ __device__ inline V3 field_one(const Prepared &p, const srs_field &f, V3 X) {
       return ld3(p.F);
     }
     case SRS_FIELD_GRID:  // grid_field with the rotation's sines and cosines precomputed
-      return grid_interp(f, p.gd, rotate_pre(X, p) - ld3(f.translation));
+      return grid_interp(f, p.gd, rotate_pre(X, p) - ld3(f.translation), p.rstep);
     default:
       return v3(0, 0, 0);
   }

@@ -121,22 +121,41 @@ __device__ inline V3 box_field(const srs_field &f, V3 X) {
   return ld3(f.field);
 }
 
+// RN(a / b) from the reciprocal rb = RN(1 / b): q = RN(a rb), r = a - b q (exact with an FMA),
+// RN(q + r rb) (P. Markstein, IBM J. Res. Dev. 34(1), 1990; normal operands, no overflow or
+// underflow).  A loop that divides by the same b many times saves the division's latency.
+__device__ __forceinline__ double div_rn(double a, double b, double rb) {
+  const double q = __dmul_rn(a, rb);
+  const double r = __fma_rn(-q, b, a);
+  return __fma_rn(r, rb, q);
+}
+
 __device__ inline V3 grid_at(const double *data, const srs_field &f, int64_t ix, int64_t iy, int64_t iz) {
   return ld3(data + 3 * (ix * f.n[1] * f.n[2] + iy * f.n[2] + iz));
 }
-__device__ inline V3 grid_lerp(V3 a, V3 b, double d, double step) { return a + (b - a) * d / step; }
+// a + (b - a) d / step, with the division as a multiply-correct sequence when the reciprocal is known
+__device__ inline V3 grid_lerp(V3 a, V3 b, double d, double step, const double *rstep, int axis) {
+  const V3 t = (b - a) * d;
+  if (rstep) {
+    const double r = rstep[axis];
+    return a + v3(div_rn(t.x, step, r), div_rn(t.y, step, r), div_rn(t.z, step, r));
+  }
+  return a + t / step;
+}
 // Interpolation at X, already in the grid's frame (rotated and translated); samples read from data
-// (the field's own array, or a copy of it in shared memory).
-__device__ inline V3 grid_interp(const srs_field &f, const double *data, V3 X) {
+// (the field's own array, or a copy of it in shared memory).  rstep (optional): 1/step per axis, for
+// the divisions by the step (same results: both are correctly rounded).
+__device__ inline V3 grid_interp(const srs_field &f, const double *data, V3 X, const double *rstep = nullptr) {
   const bool hx = f.n[0] > 1, hy = f.n[1] > 1, hz = f.n[2] > 1;
   if (hx && (X.x <= f.start[0] || X.x >= f.start[0] + (double)(f.n[0] - 1) * f.step[0])) return v3(0, 0, 0);
   if (hy && (X.y <= f.start[1] || X.y >= f.start[1] + (double)(f.n[1] - 1) * f.step[1])) return v3(0, 0, 0);
   if (hz && (X.z <= f.start[2] || X.z >= f.start[2] + (double)(f.n[2] - 1) * f.step[2])) return v3(0, 0, 0);
-  uint64_t nx = hx ? (uint64_t)((X.x - f.start[0]) / f.step[0]) : 0;
+  auto quot = [&](double a, int axis) { return rstep ? div_rn(a, f.step[axis], rstep[axis]) : a / f.step[axis]; };
+  uint64_t nx = hx ? (uint64_t)quot(X.x - f.start[0], 0) : 0;
   double dx = hx ? (X.x - f.start[0]) - (double)nx * f.step[0] : 0;
-  uint64_t ny = hy ? (uint64_t)((X.y - f.start[1]) / f.step[1]) : 0;
+  uint64_t ny = hy ? (uint64_t)quot(X.y - f.start[1], 1) : 0;
   double dy = hy ? (X.y - f.start[1]) - (double)ny * f.step[1] : 0;
-  uint64_t nz = hz ? (uint64_t)((X.z - f.start[2]) / f.step[2]) : 0;
+  uint64_t nz = hz ? (uint64_t)quot(X.z - f.start[2], 2) : 0;
   double dz = hz ? (X.z - f.start[2]) - (double)nz * f.step[2] : 0;
   // Indices stay inside the map: X is strictly inside (start, stop) on every axis with n > 1, so
   // n? <= n-2 there up to rounding of the quotient; clamp that rounding case.
@@ -144,32 +163,34 @@ __device__ inline V3 grid_interp(const srs_field &f, const double *data, V3 X) {
   if (hy && ny > (uint64_t)(f.n[1] - 2)) ny = f.n[1] - 2;
   if (hz && nz > (uint64_t)(f.n[2] - 2)) nz = f.n[2] - 2;
   const double *d = data;
+  const double *rs = rstep;
   if (hx && hy && hz) {
-    V3 v00 = grid_lerp(grid_at(d, f, nx, ny, nz), grid_at(d, f, nx + 1, ny, nz), dx, f.step[0]);
-    V3 v10 = grid_lerp(grid_at(d, f, nx, ny + 1, nz), grid_at(d, f, nx + 1, ny + 1, nz), dx, f.step[0]);
-    V3 v01 = grid_lerp(grid_at(d, f, nx, ny, nz + 1), grid_at(d, f, nx + 1, ny, nz + 1), dx, f.step[0]);
-    V3 v11 = grid_lerp(grid_at(d, f, nx, ny + 1, nz + 1), grid_at(d, f, nx + 1, ny + 1, nz + 1), dx, f.step[0]);
-    V3 v0 = grid_lerp(v00, v10, dy, f.step[1]);
-    V3 v1 = grid_lerp(v01, v11, dy, f.step[1]);
-    return grid_lerp(v0, v1, dz, f.step[2]);
+    V3 v00 = grid_lerp(grid_at(d, f, nx, ny, nz), grid_at(d, f, nx + 1, ny, nz), dx, f.step[0], rs, 0);
+    V3 v10 = grid_lerp(grid_at(d, f, nx, ny + 1, nz), grid_at(d, f, nx + 1, ny + 1, nz), dx, f.step[0], rs, 0);
+    V3 v01 = grid_lerp(grid_at(d, f, nx, ny, nz + 1), grid_at(d, f, nx + 1, ny, nz + 1), dx, f.step[0], rs, 0);
+    V3 v11 = grid_lerp(grid_at(d, f, nx, ny + 1, nz + 1), grid_at(d, f, nx + 1, ny + 1, nz + 1), dx, f.step[0], rs,
+                       0);
+    V3 v0 = grid_lerp(v00, v10, dy, f.step[1], rs, 1);
+    V3 v1 = grid_lerp(v01, v11, dy, f.step[1], rs, 1);
+    return grid_lerp(v0, v1, dz, f.step[2], rs, 2);
   } else if (hx && hy) {
-    V3 v0 = grid_lerp(grid_at(d, f, nx, ny, 0), grid_at(d, f, nx + 1, ny, 0), dx, f.step[0]);
-    V3 v1 = grid_lerp(grid_at(d, f, nx, ny + 1, 0), grid_at(d, f, nx + 1, ny + 1, 0), dx, f.step[0]);
-    return grid_lerp(v0, v1, dy, f.step[1]);
+    V3 v0 = grid_lerp(grid_at(d, f, nx, ny, 0), grid_at(d, f, nx + 1, ny, 0), dx, f.step[0], rs, 0);
+    V3 v1 = grid_lerp(grid_at(d, f, nx, ny + 1, 0), grid_at(d, f, nx + 1, ny + 1, 0), dx, f.step[0], rs, 0);
+    return grid_lerp(v0, v1, dy, f.step[1], rs, 1);
   } else if (hx && hz) {
-    V3 v0 = grid_lerp(grid_at(d, f, nx, 0, nz), grid_at(d, f, nx + 1, 0, nz), dx, f.step[0]);
-    V3 v1 = grid_lerp(grid_at(d, f, nx, 0, nz + 1), grid_at(d, f, nx + 1, 0, nz + 1), dx, f.step[0]);
-    return grid_lerp(v0, v1, dz, f.step[2]);
+    V3 v0 = grid_lerp(grid_at(d, f, nx, 0, nz), grid_at(d, f, nx + 1, 0, nz), dx, f.step[0], rs, 0);
+    V3 v1 = grid_lerp(grid_at(d, f, nx, 0, nz + 1), grid_at(d, f, nx + 1, 0, nz + 1), dx, f.step[0], rs, 0);
+    return grid_lerp(v0, v1, dz, f.step[2], rs, 2);
   } else if (hy && hz) {
-    V3 v0 = grid_lerp(grid_at(d, f, 0, ny, nz), grid_at(d, f, 0, ny + 1, nz), dy, f.step[1]);
-    V3 v1 = grid_lerp(grid_at(d, f, 0, ny, nz + 1), grid_at(d, f, 0, ny + 1, nz + 1), dy, f.step[1]);
-    return grid_lerp(v0, v1, dz, f.step[2]);
+    V3 v0 = grid_lerp(grid_at(d, f, 0, ny, nz), grid_at(d, f, 0, ny + 1, nz), dy, f.step[1], rs, 1);
+    V3 v1 = grid_lerp(grid_at(d, f, 0, ny, nz + 1), grid_at(d, f, 0, ny + 1, nz + 1), dy, f.step[1], rs, 1);
+    return grid_lerp(v0, v1, dz, f.step[2], rs, 2);
   } else if (hx) {
-    return grid_lerp(ld3(d + 3 * nx), ld3(d + 3 * (nx + 1)), dx, f.step[0]);
+    return grid_lerp(ld3(d + 3 * nx), ld3(d + 3 * (nx + 1)), dx, f.step[0], rs, 0);
   } else if (hy) {
-    return grid_lerp(ld3(d + 3 * ny), ld3(d + 3 * (ny + 1)), dy, f.step[1]);
+    return grid_lerp(ld3(d + 3 * ny), ld3(d + 3 * (ny + 1)), dy, f.step[1], rs, 1);
   } else if (hz) {
-    return grid_lerp(ld3(d + 3 * nz), ld3(d + 3 * (nz + 1)), dz, f.step[2]);
+    return grid_lerp(ld3(d + 3 * nz), ld3(d + 3 * (nz + 1)), dz, f.step[2], rs, 2);
   }
   return v3(0, 0, 0);
 }
