@@ -177,6 +177,21 @@ srs_status srs_power_density(srs_traj_view traj, srs_beam_consts beam, const dou
                              const double *d_normals, int64_t np, const srs_grid2d *grid,
                              int32_t directional, int32_t precision, double *d_out, void *stream);
 
+/* Host-buffer forms of the three sums for one particle, synchronous on the default stream: the
+ * trajectory (x, beta, aoc: HOST SoA arrays of 3*n doubles, [component][point]), points, normals and
+ * energies are HOST arrays, out (HOST) receives one value per output at weight 1.  These are what an
+ * adapter for the reference's seam calls (include/OSCARSSR_Cuda.h:26-28 copy the particle's trajectory
+ * and the surface to the device, sum, and copy back the same way).  Spectrum: precision as
+ * srs_spectrum; flux and power density: plain FP64 on any point list. */
+srs_status srs_spectrum_host(const double *x, const double *beta, int64_t n, double dt, srs_beam_consts beam,
+                             const double obs[3], const double *energies, int64_t ne, int32_t precision,
+                             double *out);
+srs_status srs_flux_host(const double *x, const double *beta, int64_t n, double dt, srs_beam_consts beam,
+                         const double *points, int64_t np, double energy_ev, double *out);
+srs_status srs_power_density_host(const double *x, const double *beta, const double *aoc, int64_t n, double dt,
+                                  srs_beam_consts beam, const double *points, const double *normals, int64_t np,
+                                  int32_t directional, double *out);
+
 /* Total radiated power of each particle (OSCARSSR.cc:1939-1978); gamma is per particle (HOST array).
  * out: HOST, nparticles values [W]. */
 srs_status srs_total_power(srs_traj_view traj, srs_beam_consts beam, const double *gamma, double *out,

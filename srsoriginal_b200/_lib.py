@@ -133,6 +133,10 @@ def _load():
         "srs_spectrum_adjoint": (S, [TrajView, BeamConsts, _D, P, C.c_int64, P, P, P, P, P]),
         "srs_trajectory_adjoint": (S, [C.POINTER(Field), C.c_int32, C.POINTER(Particle), C.c_double, C.c_double,
                                        C.c_double, C.c_int64, P, P, P, P, C.POINTER(P), _D, _D, P]),
+        "srs_spectrum_host": (S, [_D, _D, C.c_int64, C.c_double, BeamConsts, _D, _D, C.c_int64, C.c_int32, _D]),
+        "srs_flux_host": (S, [_D, _D, C.c_int64, C.c_double, BeamConsts, _D, C.c_int64, C.c_double, _D]),
+        "srs_power_density_host": (S, [_D, _D, _D, C.c_int64, C.c_double, BeamConsts, _D, _D, C.c_int64, C.c_int32,
+                                       _D]),
         "srs_energy_grid": (S, [C.c_int64, C.c_double, C.c_double, _D]),
         "srs_rectangle_plane": (S, [C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_double, _D, _D,
                                     C.c_int32, _D, _D, _D, C.POINTER(Grid2D)]),
@@ -162,7 +166,8 @@ EXPORTED = (
     "srs_sim_calculate_power_density srs_sim_calculate_total_power srs_energy_grid "
     "srs_rectangle_plane srs_rectangle_points srs_measure_peak srs_flux_mixed_noalloc "
     "srs_queue_create srs_queue_run srs_queue_info srs_queue_destroy srs_trajectory_batch "
-    "srs_spectrum_efield srs_spectrum_adjoint srs_trajectory_adjoint"
+    "srs_spectrum_efield srs_spectrum_adjoint srs_trajectory_adjoint srs_spectrum_host srs_flux_host "
+    "srs_power_density_host"
 ).split()
 
 

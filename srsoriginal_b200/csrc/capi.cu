@@ -163,6 +163,86 @@ srs_status srs_power_density(srs_traj_view traj, srs_beam_consts beam, const dou
   return SRS_OK;
 }
 
+// ---- host-buffer forms: what the reference's GPU seam does per call (copy in, sum, copy out) ----
+
+namespace {
+// Uploads a one-particle trajectory given as HOST SoA arrays (3*n each; aoc may be NULL).
+struct HostTraj {
+  DeviceBuffer buf;
+  srs_traj_view view{};
+  srs_status up(const double *x, const double *beta, const double *aoc, int64_t n, double dt, cudaStream_t s) {
+    if (!x || !beta || n < 1) return fail(SRS_ERR_INVALID, "bad trajectory");
+    const size_t arr = sizeof(double) * 3 * (size_t)n;
+    SRS_CUDA(buf.alloc(arr * (aoc ? 3 : 2), s));
+    double *d = buf.as<double>();
+    SRS_CUDA(cudaMemcpyAsync(d, x, arr, cudaMemcpyHostToDevice, s));
+    SRS_CUDA(cudaMemcpyAsync(d + 3 * n, beta, arr, cudaMemcpyHostToDevice, s));
+    if (aoc) SRS_CUDA(cudaMemcpyAsync(d + 6 * n, aoc, arr, cudaMemcpyHostToDevice, s));
+    view = srs_traj_view{d, d + 3 * n, aoc ? d + 6 * n : nullptr, n, 1, dt};
+    return SRS_OK;
+  }
+};
+srs_status upload(DeviceBuffer &b, const double *h, size_t count, cudaStream_t s) {
+  SRS_CUDA(b.alloc(sizeof(double) * std::max<size_t>(1, count), s));
+  if (count) SRS_CUDA(cudaMemcpyAsync(b.ptr, h, sizeof(double) * count, cudaMemcpyHostToDevice, s));
+  return SRS_OK;
+}
+srs_status download(double *h, const DeviceBuffer &b, size_t count, cudaStream_t s) {
+  SRS_CUDA(cudaMemcpyAsync(h, b.ptr, sizeof(double) * count, cudaMemcpyDeviceToHost, s));
+  SRS_CUDA(cudaStreamSynchronize(s));
+  return SRS_OK;
+}
+}  // namespace
+
+srs_status srs_spectrum_host(const double *x, const double *beta, int64_t n, double dt, srs_beam_consts beam,
+                             const double obs[3], const double *energies, int64_t ne, int32_t precision,
+                             double *out) {
+  clear_error();
+  if (!energies || !out || !obs || ne < 1) return fail(SRS_ERR_INVALID, "bad argument");
+  cudaStream_t s = nullptr;
+  HostTraj t;
+  DeviceBuffer de, dout;
+  if (srs_status st = t.up(x, beta, nullptr, n, dt, s)) return st;
+  if (srs_status st = upload(de, energies, ne, s)) return st;
+  SRS_CUDA(dout.alloc(sizeof(double) * ne, s));
+  if (srs_status st = srs_spectrum(t.view, beam, obs, de.as<double>(), ne, precision, dout.as<double>(), s)) return st;
+  return download(out, dout, ne, s);
+}
+
+srs_status srs_flux_host(const double *x, const double *beta, int64_t n, double dt, srs_beam_consts beam,
+                         const double *points, int64_t np, double energy_ev, double *out) {
+  clear_error();
+  if (!points || !out || np < 1) return fail(SRS_ERR_INVALID, "bad argument");
+  cudaStream_t s = nullptr;
+  HostTraj t;
+  DeviceBuffer dp, dout;
+  if (srs_status st = t.up(x, beta, nullptr, n, dt, s)) return st;
+  if (srs_status st = upload(dp, points, 3 * np, s)) return st;
+  SRS_CUDA(dout.alloc(sizeof(double) * np, s));
+  if (srs_status st = srs_flux(t.view, beam, dp.as<double>(), np, nullptr, energy_ev, SRS_PRECISION_FP64,
+                               dout.as<double>(), s))
+    return st;
+  return download(out, dout, np, s);
+}
+
+srs_status srs_power_density_host(const double *x, const double *beta, const double *aoc, int64_t n, double dt,
+                                  srs_beam_consts beam, const double *points, const double *normals, int64_t np,
+                                  int32_t directional, double *out) {
+  clear_error();
+  if (!points || !normals || !out || !aoc || np < 1) return fail(SRS_ERR_INVALID, "bad argument");
+  cudaStream_t s = nullptr;
+  HostTraj t;
+  DeviceBuffer dp, dn, dout;
+  if (srs_status st = t.up(x, beta, aoc, n, dt, s)) return st;
+  if (srs_status st = upload(dp, points, 3 * np, s)) return st;
+  if (srs_status st = upload(dn, normals, 3 * np, s)) return st;
+  SRS_CUDA(dout.alloc(sizeof(double) * np, s));
+  if (srs_status st = srs_power_density(t.view, beam, dp.as<double>(), dn.as<double>(), np, nullptr, directional,
+                                        SRS_PRECISION_FP64, dout.as<double>(), s))
+    return st;
+  return download(out, dout, np, s);
+}
+
 srs_status srs_total_power(srs_traj_view traj, srs_beam_consts beam, const double *gamma, double *out, void *stream) {
   clear_error();
   if (srs_status st = check_view(traj, true)) return st;

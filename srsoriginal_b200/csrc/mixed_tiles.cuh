@@ -16,13 +16,46 @@ namespace tiles {
 constexpr int kThreads = 128;
 constexpr int kTileA = 8, kTileB = 16;  // points of a CTA tile along u1 and u2 (kTileA * kTileB == kThreads)
 constexpr int kSub = 128;               // trajectory points per shared-memory tile
-constexpr int kTargetCtas = 148 * 6;
 constexpr int kEnergiesPerThread = 4;
 
-inline int splits_for(int64_t ctas, int64_t n, int64_t min_chunk) {
-  int64_t s = (kTargetCtas + ctas - 1) / std::max<int64_t>(1, ctas);
-  int64_t max_s = std::max<int64_t>(1, n / min_chunk);
-  return (int)std::min<int64_t>(std::max<int64_t>(1, std::min(s, max_s)), 65535);
+// Trajectory chunks S per tile for ctas tiles on a GPU with `slots` resident CTAs per wave: the S
+// minimising the modelled time waves(S) * (n/S + overhead), waves = ceil(ctas * S / slots), with
+// chunks of at least min_chunk points.  A grid that overshoots a whole wave by a few CTAs leaves them
+// to run alone at the end, so the model picks S that fills the last wave instead.
+inline int splits_for(int64_t ctas, int64_t n, int64_t min_chunk, int64_t slots) {
+  ctas = std::max<int64_t>(1, ctas);
+  slots = std::max<int64_t>(1, slots);
+  const int64_t max_s = std::min<int64_t>(std::max<int64_t>(1, n / min_chunk), 4096);
+  constexpr double kOverhead = 64.0;  // per-CTA set-up and output, in trajectory points
+  int best_s = 1;
+  double best = 1e300;
+  for (int64_t s = 1; s <= max_s; ++s) {
+    const int64_t waves = (ctas * s + slots - 1) / slots;
+    const double cost = (double)waves * ((double)((n + s - 1) / s) + kOverhead);
+    if (cost < best * (1.0 - 1e-9)) {
+      best = cost;
+      best_s = (int)s;
+    }
+  }
+  return best_s;
+}
+
+// Trajectory points per chunk for S chunks, rounded up to whole shared-memory sub-tiles: the FP32
+// accumulators restart at every sub-tile, so with sub-tile-aligned chunks the result depends on S
+// only through the FP64 order of the per-chunk sums.  The chunks actually used are ceil(n / chunk).
+inline int64_t aligned_chunk(int64_t n, int S) {
+  const int64_t c = (n + S - 1) / std::max(1, S);
+  return (c + kSub - 1) / kSub * kSub;
+}
+inline int used_chunks(int64_t n, int64_t chunk) { return (int)((n + chunk - 1) / chunk); }
+
+// Resident CTAs of `kernel` (kThreads threads, no dynamic shared memory) on the current device.
+template <typename K>
+inline int64_t wave_slots(K kernel) {
+  int dev = 0, sms = 148, occ = 1;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kThreads, 0) != cudaSuccess || occ < 1) occ = 1;
+  return (int64_t)sms * occ;
 }
 
 struct GridTiles {

@@ -142,6 +142,7 @@ srs_status srs_queue_create(srs_queue **out, const srs_job *jobs, int32_t njobs,
   clear_error();
   if (!out || !jobs || njobs < 1) return fail(SRS_ERR_INVALID, "no jobs");
   if (chunk < 128) return fail(SRS_ERR_INVALID, "chunk must be >= 128 trajectory points");
+  chunk = (int32_t)aligned_chunk(chunk, 1);  // whole shared-memory sub-tiles (see aligned_chunk)
   std::unique_ptr<srs_queue> q(new srs_queue());
   std::vector<QJob> hj(njobs);
   std::vector<int64_t> offsets(njobs + 1, 0);

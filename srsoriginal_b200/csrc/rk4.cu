@@ -163,14 +163,16 @@ __device__ void stage_grids(const srs_field *sf, Prepared *sp, int nfields) {
 // With specs != nullptr each particle has its own time step, point counts and output arrays (jobs of
 // different trajectory lengths); a warp then runs its longest particle's step count, and groups whose
 // trajectory is complete keep stepping without storing.
+template <int G>
 __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restrict__ gfields, int nfields,
                                                        const srs_particle *__restrict__ particles, int nparticles,
-                                                       double dt_all, int64_t nfwd_all, int64_t nbwd_all, int G,
+                                                       double dt_all, int64_t nfwd_all, int64_t nbwd_all,
                                                        double *__restrict__ X, double *__restrict__ Bt,
                                                        double *__restrict__ A, const TrajSpec *__restrict__ specs,
                                                        int64_t stage_doubles) {
   __shared__ srs_field sf[kMaxFieldsShared];
   __shared__ Prepared sp[kMaxFieldsShared];
+  __shared__ double sink[128];  // target of the stores a lane does not make (no branch around them)
   for (int i = threadIdx.x; i < nfields; i += blockDim.x) {
     sf[i] = gfields[i];
     prepare(sf[i], sp[i]);
@@ -194,15 +196,16 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
     fmax = max(fmax, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)fmax, o));
     bmax = max(bmax, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)bmax, o));
   }
-  const int slot = nfields > 0 ? gl / nfields : 2, fidx = nfields > 0 ? gl % nfields : 0;
-  const bool evaluates = slot < 2;
+  // lane gl evaluates field gl % nfields at position (gl / nfields) % 2; lanes past 2 * nfields
+  // repeat an evaluation (their results are not read), so no lane branches around the evaluation
+  const int slot = nfields > 0 ? (gl / nfields) & 1 : 0, fidx = nfields > 0 ? gl % nfields : 0;
   const double C = kC, qomg = P.qomg;
   const unsigned full = 0xffffffffu;
 
   // B at two positions, one per slot, summed over fields in field order
   auto fields2 = [&](V3 pa, V3 pb, V3 &Ba, V3 &Bb) {
     V3 mine = v3(0, 0, 0);
-    if (evaluates) mine = field_one(sp[fidx], sf[fidx], slot == 0 ? pa : pb);
+    if (nfields > 0) mine = field_one(sp[fidx], sf[fidx], slot == 0 ? pa : pb);
     Ba = v3(0, 0, 0);
     Bb = v3(0, 0, 0);
     for (int f = 0; f < nfields; ++f) {
@@ -214,13 +217,15 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   // the group's lanes store the nine components of a point (x, y, z, beta = v/c, a/c), lane gl taking
   // components gl, gl + G, ...; selects, not branches
   const double rC = 1.0 / C;
-  auto store = [&](int64_t k, V3 pos, V3 vel, V3 acc) {
-    if (!owner) return;
-    for (int c = gl; c < 9; c += G) {
+  double *const my_sink = sink + (threadIdx.x & 127);
+  auto store = [&](int64_t k, bool keep, V3 pos, V3 vel, V3 acc) {
+#pragma unroll
+    for (int r = 0; r < (9 + G - 1) / G; ++r) {
+      const int c = gl + r * G;
       const int l3 = c < 3 ? c : c < 6 ? c - 3 : c - 6;
       const V3 src = c < 3 ? pos : c < 6 ? vel : acc;
       const double v = l3 == 0 ? src.x : l3 == 1 ? src.y : src.z;
-      double *const o = (c < 3 ? xp : c < 6 ? bp : ap) + (int64_t)l3 * n + k;
+      double *const o = (keep && owner && c < 9) ? (c < 3 ? xp : c < 6 ? bp : ap) + (int64_t)l3 * n + k : my_sink;
       *o = c < 3 ? v : div_rn(v, C, rC);
     }
   };
@@ -256,7 +261,7 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   const V3 vel0 = v3(P.beta0[0] * C, P.beta0[1] * C, P.beta0[2] * C);
   V3 pos = pos0, vel = vel0, acc = v3(0, 0, 0);
   for (int64_t i = 0; i < fmax; ++i) {
-    if (i < nfwd) store(nbwd + i, pos, vel, acc);
+    store(nbwd + i, i < nfwd, pos, vel, acc);
     acc = step(pos, vel, dt);
   }
   pos = pos0;
@@ -264,7 +269,7 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   const double mdt = -dt;
   for (int64_t i = 0; i < bmax; ++i) {
     acc = step(pos, vel, mdt);
-    if (i < nbwd) store(nbwd - 1 - i, pos, vel, acc);
+    store(nbwd - 1 - i, i < nbwd, pos, vel, acc);
   }
 }
 
@@ -377,6 +382,36 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 }
 }  // namespace
 
+template <int G>
+static cudaError_t launch_warp_rk4_g(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
+                              double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
+                              const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s) {
+  const size_t smem = sizeof(double) * (size_t)stage_doubles;
+  if (cudaError_t e = allow_smem(rk4_warp_kernel<G>, smem)) return e;
+  const int warps = 4, per_block = warps * (32 / G);
+  rk4_warp_kernel<G><<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
+      d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, d_specs, stage_doubles);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_warp_rk4(int G, const srs_field *d_fields, int nfields, const srs_particle *d_particles,
+                            int nparticles, double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b,
+                            double *d_a, const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s) {
+  switch (G) {
+    case 2: return launch_warp_rk4_g<2>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+                                        d_specs, stage_doubles, s);
+    case 4: return launch_warp_rk4_g<4>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+                                        d_specs, stage_doubles, s);
+    case 8: return launch_warp_rk4_g<8>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+                                        d_specs, stage_doubles, s);
+    case 16: return launch_warp_rk4_g<16>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+                                          d_specs, stage_doubles, s);
+    case 32: return launch_warp_rk4_g<32>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+                                          d_specs, stage_doubles, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
                        double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
                        cudaStream_t s, int64_t stage_doubles) {
@@ -387,10 +422,9 @@ cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particl
   // grouped lanes while there are few particles per SM (the serial chain is the limit); one thread
   // per particle when there are enough particles to fill the SMs (issue rate is the limit)
   if (G <= 32 && (int64_t)nparticles * G <= 148 * 32 * 48) {
-    const int warps = 4, per_block = warps * (32 / G);
-    if (cudaError_t e = allow_smem(rk4_warp_kernel, smem)) return e;
-    rk4_warp_kernel<<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
-        d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, G, d_x, d_b, d_a, nullptr, stage_doubles);
+    if (cudaError_t e = launch_warp_rk4(G, d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+                                        nullptr, stage_doubles, s))
+      return e;
   } else {
     const int threads = 64;
     if (cudaError_t e = allow_smem(rk4_thread_kernel, smem)) return e;
@@ -406,11 +440,9 @@ cudaError_t launch_rk4_specs(const srs_field *d_fields, int nfields, const srs_p
   if (nfields > kMaxFieldsShared) return cudaErrorInvalidValue;
   const int G = group_size(nparticles, nfields);
   if (G > 32) return cudaErrorInvalidValue;
-  const size_t smem = sizeof(double) * (size_t)stage_doubles;
-  if (cudaError_t e = allow_smem(rk4_warp_kernel, smem)) return e;
-  const int warps = 4, per_block = warps * (32 / G);
-  rk4_warp_kernel<<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
-      d_fields, nfields, d_particles, nparticles, 0.0, 0, 0, G, nullptr, nullptr, nullptr, d_specs, stage_doubles);
+  if (cudaError_t e = launch_warp_rk4(G, d_fields, nfields, d_particles, nparticles, 0.0, 0, 0, nullptr, nullptr,
+                                      nullptr, d_specs, stage_doubles, s))
+    return e;
   return cudaGetLastError();
 }
 

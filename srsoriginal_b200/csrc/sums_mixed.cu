@@ -172,7 +172,7 @@ __global__ void omega_kernel(const double *__restrict__ e, int64_t ne, double *_
 
 static int flux_mixed_splits(int64_t n, const srs_grid2d &g, int nparticles) {
   GridTiles t = tiles_of(g);
-  return splits_for((int64_t)t.t1 * t.t2 * nparticles, n, 512);
+  return splits_for((int64_t)t.t1 * t.t2 * nparticles, n, 256, wave_slots(flux_mixed_kernel));
 }
 
 size_t mixed_flux_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles) {
@@ -180,8 +180,9 @@ size_t mixed_flux_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles) 
 }
 
 static cudaError_t mixed_flux_splits(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g,
-                                     double energy_ev, double *d_out, void *scratch, int S, cudaStream_t s) {
-  const int64_t chunk = (t.n + S - 1) / S;
+                                     double energy_ev, double *d_out, void *scratch, int S_max, cudaStream_t s) {
+  const int64_t chunk = aligned_chunk(t.n, S_max);
+  const int S = used_chunks(t.n, chunk);
   GridTiles tl = tiles_of(g);
   const double omega = ev_to_omega(energy_ev);
   double *partial = static_cast<double *>(scratch);
@@ -266,14 +267,15 @@ namespace srs {
 size_t mixed_pd_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles) {
   GridTiles tl = tiles_of(g);
   return sizeof(double) * (size_t)g.n1 * g.n2 * nparticles *
-         splits_for((int64_t)tl.t1 * tl.t2 * nparticles, n, 512);
+         splits_for((int64_t)tl.t1 * tl.t2 * nparticles, n, 256, wave_slots(pd_mixed_kernel));
 }
 
 cudaError_t mixed_power_density(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g,
                                 int directional, double *d_out, void *scratch, cudaStream_t s) {
   GridTiles tl = tiles_of(g);
-  const int S = splits_for((int64_t)tl.t1 * tl.t2 * t.nparticles, t.n, 512);
-  const int64_t chunk = (t.n + S - 1) / S;
+  const int64_t chunk =
+      aligned_chunk(t.n, splits_for((int64_t)tl.t1 * tl.t2 * t.nparticles, t.n, 256, wave_slots(pd_mixed_kernel)));
+  const int S = used_chunks(t.n, chunk);
   double *partial = static_cast<double *>(scratch);
   dim3 grid((unsigned)(tl.t1 * tl.t2), S, t.nparticles);
   pd_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.aoc, t.n, g, g.normal[0], g.normal[1], g.normal[2], directional, chunk,
@@ -286,17 +288,18 @@ cudaError_t mixed_power_density(const srs_traj_view &t, const srs_beam_consts &b
 
 size_t mixed_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles) {
   const int64_t ctas = (ne + kThreads * kEnergiesPerThread - 1) / (kThreads * kEnergiesPerThread) * nparticles;
-  return sizeof(double) * ((size_t)6 * ne * nparticles * splits_for(ctas, n, 256) + ne);
+  return sizeof(double) * ((size_t)6 * ne * nparticles * splits_for(ctas, n, 256, wave_slots(spectrum_mixed_kernel)) + ne);
 }
 
 cudaError_t mixed_spectrum(const srs_traj_view &t, const srs_beam_consts &b, const double obs[3],
                            const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s,
                            double *d_e6) {
   const int64_t etiles = (ne + kThreads * kEnergiesPerThread - 1) / (kThreads * kEnergiesPerThread);
-  const int S = splits_for(etiles * t.nparticles, t.n, 256);
-  const int64_t chunk = (t.n + S - 1) / S;
+  const int S_max = splits_for(etiles * t.nparticles, t.n, 256, wave_slots(spectrum_mixed_kernel));
+  const int64_t chunk = aligned_chunk(t.n, S_max);
+  const int S = used_chunks(t.n, chunk);
   double *partial = static_cast<double *>(scratch);
-  double *omegas = partial + (size_t)6 * ne * t.nparticles * S;
+  double *omegas = partial + (size_t)6 * ne * t.nparticles * S_max;  // after the S_max chunks sized for
   omega_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(d_energies, ne, omegas);
   dim3 grid((unsigned)etiles, S, t.nparticles);
   spectrum_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt, v3(obs[0], obs[1], obs[2]), omegas, ne,

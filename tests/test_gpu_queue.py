@@ -57,7 +57,7 @@ def test_queue_matches_one_shot(small_specs):
         torch.cuda.synchronize()
         ref, ref64 = ref.cpu().numpy(), ref64.cpu().numpy()
         assert np.all(np.isfinite(got))
-        assert _rel(got, ref) <= 1e-5, s            # same arithmetic, other chunking
+        assert _rel(got, ref) <= 1e-12, s           # same sub-tile sums, other chunk grouping
         assert _rel(got, ref64) <= 1e-4, s          # mixed vs plain FP64
     # a second run of the captured graph gives the same numbers (deterministic reduction)
     first = [keep[-1].clone() for _, keep in jobs]
