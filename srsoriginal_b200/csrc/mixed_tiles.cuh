@@ -90,8 +90,25 @@ __device__ inline Anchor make_anchor(const double Oc[3], const double *xp, const
 }
 
 
+// Packed FP32x2 arithmetic (sm_100): one instruction performs the same operation on two values, each
+// rounded as the scalar operation would be.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+// Per trajectory point, 13 FP32 values anchored at the tile centre, stored for PAIRS of consecutive
+// points: record g of pair q is (field 2g of point 2q, of point 2q+1, field 2g+1 of 2q, of 2q+1), so
+// one 16-byte broadcast load yields two fields of both points, ready for the packed instructions.
+//   0 phase (turns, mod 1)        1 k1 (turns per grid step along u1, mod 1)
+//   2 k2 (along u2)               3 (w/c)/(2 D_c)/2pi (turns per m^2)
+//   4-6 n_c                       7 1/(2 D_c)
+//   8 1/D_c                       9-11 (n_c - bhat) + bhat (1 - |beta|)
+//   12 near-field z term -(c/w) n_cz / D_c^2          (13: padding)
+constexpr int kFluxFields = 14;
 struct FluxShared {
-  float4 r[4][kSub];
+  float4 r[kFluxFields / 2][kSub / 2];
 };
 
 // Flux: one tile of kTileA x kTileB grid points (tile T1, T2) against trajectory points [i0, iend);
@@ -100,17 +117,13 @@ struct FluxShared {
 __device__ __forceinline__ void flux_tile(const double *__restrict__ xp, const double *__restrict__ bp, int64_t n,
                                           double dt, const srs_grid2d &g, double omega, int T1, int T2, int64_t i0,
                                           int64_t iend, double *__restrict__ out6, FluxShared &sh) {
-  // Per trajectory point i (anchored at the tile centre), five float4 records read as broadcasts:
-  //   r0 = (phase mod 1 turn, k1, k2 [turns per grid step, mod 1], (w/c)/(2 D_c) / 2pi [turns per m^2])
-  //   r1 = (n_c, 1/D_c)
-  //   r2 = ((n_c - bhat) + bhat (1 - |beta|), near-field z term -(c/w) n_cz / D_c^2)
-  //   r3 = (1/(2 D_c), unused x3)
-  // Phases are kept in turns so that the reduction to [-1/2, 1/2) is exact (x - rint(x)).
+  // Phases are kept in turns so that the reduction to [-1/2, 1/2) is exact (x - rint(x), rint by
+  // the 1.5 * 2^23 shift, exact for |x| < 2^22 turns).
   // Terms below FP32 resolution are dropped: the third-order distance term g (|Delta|^2 - g^2)/(2 D_c^2)
   // (< 1e-7 rad here) and the near-field term's x, y parts (relative size lambda/(2 pi D) times
   // n_perp, < 1e-10 at 30 m); 1/D_j = (1/D_c)(1 - (D_j - D_c)/D_c) to first order (relative error
   // ((D_j - D_c)/D_c)^2 < 1e-16).
-  float4 (*sm)[kSub] = sh.r;
+  float *rec = &sh.r[0][0].x;
   const int tid = threadIdx.x;
   const int a = tid / kTileB, b = tid % kTileB;
   const int i1 = T1 * kTileA + a, i2 = T2 * kTileB + b;
@@ -124,12 +137,16 @@ __device__ __forceinline__ void flux_tile(const double *__restrict__ xp, const d
   const int da = i1 - ca, db = i2 - cb;
   float Dl[3];
   for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);
-  const float dd = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
-  const float fda = (float)da, fdb = (float)db;
+  const float2 Dx = f2(Dl[0], Dl[0]), Dy = f2(Dl[1], Dl[1]), Dz = f2(Dl[2], Dl[2]);
+  const float ddv = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
+  const float2 dd = f2(ddv, ddv), fda = f2((float)da, (float)da), fdb = f2((float)db, (float)db);
+  const float2 shift = f2(12582912.0f, 12582912.0f), two_pi = f2(6.28318530717958647692f, 6.28318530717958647692f);
   const double wc = omega / kC;
   const double inv2pi = 0.15915494309189535;
-  const float two_pi_f = 6.28318530717958647692f;
   double E[6] = {0, 0, 0, 0, 0, 0};
+
+  // slot of field f of point t (t < kSub) in the pair-packed records
+  auto put = [&](int t, int f, float v) { rec[((f >> 1) * (kSub / 2) + (t >> 1)) * 4 + (f & 1) * 2 + (t & 1)] = v; };
 
   for (int64_t base = i0; base < iend; base += kSub) {
     const int cnt = (int)imin64(kSub, iend - base);
@@ -140,42 +157,63 @@ __device__ __forceinline__ void flux_tile(const double *__restrict__ xp, const d
       const double tau = dt * (double)i + A.Dc / kC;
       const double k1 = reduce_2pi(wc * (A.nc[0] * g.u1[0] + A.nc[1] * g.u1[1] + A.nc[2] * g.u1[2]));
       const double k2 = reduce_2pi(wc * (A.nc[0] * g.u2[0] + A.nc[1] * g.u2[1] + A.nc[2] * g.u2[2]));
-      sm[0][tid] = make_float4((float)(reduce_2pi(omega * tau) * inv2pi), (float)(k1 * inv2pi), (float)(k2 * inv2pi),
-                               (float)(wc * 0.5 * A.invDc * inv2pi));
-      sm[1][tid] = make_float4((float)A.nc[0], (float)A.nc[1], (float)A.nc[2], (float)A.invDc);
-      sm[2][tid] = make_float4((float)(A.dc[0] + A.bhat[0] * A.omb), (float)(A.dc[1] + A.bhat[1] * A.omb),
-                               (float)(A.dc[2] + A.bhat[2] * A.omb),
-                               (float)(-(kC / omega) * A.invDc * A.invDc * A.nc[2]));
-      sm[3][tid] = make_float4((float)(0.5 * A.invDc), 0.f, 0.f, 0.f);
+      put(tid, 0, (float)(reduce_2pi(omega * tau) * inv2pi));
+      put(tid, 1, (float)(k1 * inv2pi));
+      put(tid, 2, (float)(k2 * inv2pi));
+      put(tid, 3, (float)(wc * 0.5 * A.invDc * inv2pi));
+      put(tid, 4, (float)A.nc[0]);
+      put(tid, 5, (float)A.nc[1]);
+      put(tid, 6, (float)A.nc[2]);
+      put(tid, 7, (float)(0.5 * A.invDc));
+      put(tid, 8, (float)A.invDc);
+      put(tid, 9, (float)(A.dc[0] + A.bhat[0] * A.omb));
+      put(tid, 10, (float)(A.dc[1] + A.bhat[1] * A.omb));
+      put(tid, 11, (float)(A.dc[2] + A.bhat[2] * A.omb));
+      put(tid, 12, (float)(-(kC / omega) * A.invDc * A.invDc * A.nc[2]));
+    } else if (tid == cnt && (cnt & 1)) {
+      // the odd count's partner slot: all zero, so 1/D_j = 0 and its amplitude and near-field term vanish
+      for (int f = 0; f < 13; ++f) put(tid, f, 0.0f);
     }
     __syncthreads();
     if (!active) continue;
-    float e0 = 0, e1 = 0, e2 = 0, e3 = 0, e4 = 0, e5 = 0;
-#pragma unroll 4
-    for (int k = 0; k < cnt; ++k) {
-      const float4 r0 = sm[0][k], r1 = sm[1][k], r2 = sm[2][k];
-      const float hinv = sm[3][k].x;
-      const float gq = fmaf(r1.z, Dl[2], fmaf(r1.y, Dl[1], r1.x * Dl[0]));  // n_c . Delta
-      const float h = fmaf(-gq, gq, dd);                                    // |Delta|^2 - g^2
-      const float del = fmaf(h, hinv, gq);                                  // D_j - D_c
-      const float t = del * r1.w;
-      const float rinv = fmaf(-t, r1.w, r1.w);                              // 1/D_j
-      float ph = fmaf(r0.y, fda, r0.x);
-      ph = fmaf(r0.z, fdb, ph);
-      ph = fmaf(h, r0.w, ph);                                               // turns
-      const float fr = ph - rintf(ph);
-      float sn, cs;
-      __sincosf(fr * two_pi_f, &sn, &cs);
-      // amplitude (beta - n_j)/D_j = -((n_c - bhat + bhat omb) + (Delta - n_c del)/D_j)/D_j
-      const float ux = fmaf(fmaf(-r1.x, del, Dl[0]), rinv, r2.x);
-      const float uy = fmaf(fmaf(-r1.y, del, Dl[1]), rinv, r2.y);
-      const float uz = fmaf(fmaf(-r1.z, del, Dl[2]), rinv, r2.z);
-      const float ax = ux * rinv, ay = uy * rinv, az = uz * rinv;  // minus the amplitude
-      e0 = fmaf(-ax, cs, e0); e1 = fmaf(-ax, sn, e1);
-      e2 = fmaf(-ay, cs, e2); e3 = fmaf(-ay, sn, e3);
-      e4 = fmaf(-az, cs, fmaf(-r2.w, sn, e4)); e5 = fmaf(-az, sn, fmaf(r2.w, cs, e5));
+    float2 acc[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[c] = f2(0.f, 0.f);
+    const int pairs = (cnt + 1) >> 1;
+#pragma unroll 2
+    for (int q = 0; q < pairs; ++q) {
+      const float4 R0 = sh.r[0][q], R1 = sh.r[1][q], R2 = sh.r[2][q], R3 = sh.r[3][q], R4 = sh.r[4][q],
+                   R5 = sh.r[5][q], R6 = sh.r[6][q];
+      const float2 ph0 = f2(R0.x, R0.y), k1 = f2(R0.z, R0.w), k2 = f2(R1.x, R1.y), qc = f2(R1.z, R1.w);
+      const float2 nx = f2(R2.x, R2.y), ny = f2(R2.z, R2.w), nz = f2(R3.x, R3.y), hinv = f2(R3.z, R3.w);
+      const float2 w = f2(R4.x, R4.y), bx = f2(R4.z, R4.w), by = f2(R5.x, R5.y), bz = f2(R5.z, R5.w);
+      const float2 nf = f2(R6.x, R6.y);
+      const float2 gq = fma2(nz, Dz, fma2(ny, Dy, mul2(nx, Dx)));  // n_c . Delta
+      const float2 h = fma2(neg2(gq), gq, dd);                     // |Delta|^2 - g^2
+      const float2 del = fma2(h, hinv, gq);                        // D_j - D_c
+      const float2 t = mul2(del, w);
+      const float2 rinv = fma2(neg2(t), w, w);                     // 1/D_j
+      float2 ph = fma2(k1, fda, ph0);
+      ph = fma2(k2, fdb, ph);
+      ph = fma2(h, qc, ph);                                        // turns
+      const float2 fr = add2(ph, neg2(add2(add2(ph, shift), neg2(shift))));
+      const float2 x = mul2(fr, two_pi);
+      float2 sn, cs;
+      __sincosf(x.x, &sn.x, &cs.x);
+      __sincosf(x.y, &sn.y, &cs.y);
+      // minus the amplitude: ((n_c - bhat + bhat omb) + (Delta - n_c del)/D_j)/D_j
+      const float2 ax = mul2(fma2(fma2(neg2(nx), del, Dx), rinv, bx), rinv);
+      const float2 ay = mul2(fma2(fma2(neg2(ny), del, Dy), rinv, by), rinv);
+      const float2 az = mul2(fma2(fma2(neg2(nz), del, Dz), rinv, bz), rinv);
+      acc[0] = fma2(neg2(ax), cs, acc[0]);
+      acc[1] = fma2(neg2(ax), sn, acc[1]);
+      acc[2] = fma2(neg2(ay), cs, acc[2]);
+      acc[3] = fma2(neg2(ay), sn, acc[3]);
+      acc[4] = fma2(neg2(az), cs, fma2(neg2(nf), sn, acc[4]));
+      acc[5] = fma2(neg2(az), sn, fma2(nf, cs, acc[5]));
     }
-    E[0] += e0; E[1] += e1; E[2] += e2; E[3] += e3; E[4] += e4; E[5] += e5;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) E[c] += (double)acc[c].x + (double)acc[c].y;
   }
   if (active) {
     double *o = out6 + j;
