@@ -256,7 +256,11 @@ def measure_configs(dev):
     msm = _events_ms(lambda: D.power_density(t2, charge, current, pd, grid=g2, precision=_lib.MIXED), 5)
     ms = _events_ms(lambda: D.power_density(t2, charge, current, pd64, points=pts, normals=nrms,
                                             precision=_lib.FP64), 2)
-    a, b = pd.cpu().numpy(), pd64.cpu().numpy()
+    # accuracy from fresh outputs, after the timed calls
+    chk, chk64 = torch.zeros_like(pd), torch.zeros_like(pd64)
+    D.power_density(t2, charge, current, chk, grid=g2, precision=_lib.MIXED)
+    D.power_density(t2, charge, current, chk64, points=pts, normals=nrms, precision=_lib.FP64)
+    a, b = chk.cpu().numpy(), chk64.cpu().numpy()
     ev = 40001 * 201 * 201
     out["cfg2_power_density"] = {"evals": ev, "mixed_ms": msm, "mixed_evals_per_s": ev / (msm * 1e-3),
                                  "fp64_ms": ms, "fp64_evals_per_s": ev / (ms * 1e-3),

@@ -225,7 +225,7 @@ __device__ __forceinline__ void flux_tile(const double *__restrict__ xp, const d
 
 struct SpecShared {
   double tau[kSub];
-  float v[8][kSub];
+  float v[10][kSub];
 };
 
 // Each thread owns kEnergiesPerThread consecutive energies.  The rotation exp(i dw tau_i) is shared by
@@ -239,7 +239,7 @@ __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, con
                                               int64_t ne, int etile, int64_t i0, int64_t iend,
                                               double *__restrict__ out6, SpecShared &sh) {
   double *stau = sh.tau;
-  float (*sv)[kSub] = sh.v;  // a = (beta - n)/D (3), b' = n/D^2 (3), rotation exp(i dw tau) (2)
+  float (*sv)[kSub] = sh.v;  // a = (beta - n)/D (3), b' = n/D^2 (3), exp(i dw tau) (2), exp(2 i dw tau) (2)
   constexpr int K = kEnergiesPerThread;
   const int tid = threadIdx.x;
   const int64_t k0 = ((int64_t)etile * kThreads + tid) * K;
@@ -257,6 +257,10 @@ __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, con
     const double dev = fabs(wk[q] - (wfirst + (double)k * dw));
     if (k0 + q < ne && dev * (1e3 / kC) >= 1e-3) uniform = false;  // observers within 1 km
   }
+  static_assert(K % 2 == 0, "energies per thread come in pairs");
+  float2 kap2[K / 2];
+#pragma unroll
+  for (int pq = 0; pq < K / 2; ++pq) kap2[pq] = f2(kap[2 * pq], kap[2 * pq + 1]);
   double E[K][6];
 #pragma unroll
   for (int q = 0; q < K; ++q)
@@ -284,43 +288,72 @@ __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, con
       sincos(reduce_2pi(dw * tau), &sr, &cr);
       sv[6][tid] = (float)cr;
       sv[7][tid] = (float)sr;
+      sincos(reduce_2pi(2.0 * dw * tau), &sr, &cr);  // the rotation by two energy steps
+      sv[8][tid] = (float)cr;
+      sv[9][tid] = (float)sr;
     }
     __syncthreads();
     if (!active) continue;
-    float e[K][6];
+    // accumulators packed by energy pairs (q, q+1): acc[p][c] = (e[2p][c], e[2p+1][c])
+    float2 acc[K / 2][6];
 #pragma unroll
-    for (int q = 0; q < K; ++q)
+    for (int pq = 0; pq < K / 2; ++pq)
 #pragma unroll
-      for (int c = 0; c < 6; ++c) e[q][c] = 0;
+      for (int c = 0; c < 6; ++c) acc[pq][c] = f2(0.f, 0.f);
     for (int k = 0; k < cnt; ++k) {
       const double tau = stau[k];
       const float ax = sv[0][k], ay = sv[1][k], az = sv[2][k];
       const float bx = sv[3][k], by = sv[4][k], bz = sv[5][k];
       const float rr = sv[6][k], ri = sv[7][k];
-      float zr, zi;
-      __sincosf((float)reduce_2pi(wk[0] * tau), &zi, &zr);
+      // z_q = exp(i w_q tau): z_0 from one reduced sincos, then the rotation exp(i dw tau) on a uniform
+      // grid (z_{q+1} = z_q rot for the first pair, the pair times rot^2 for the next), else sincos
+      float2 zr[K / 2], zi[K / 2];
+      float z0r, z0i;
+      __sincosf((float)reduce_2pi(wk[0] * tau), &z0i, &z0r);
+      if (uniform) {
+        const float z1r = z0r * rr - z0i * ri, z1i = fmaf(z0r, ri, z0i * rr);
+        zr[0] = f2(z0r, z1r);
+        zi[0] = f2(z0i, z1i);
+        const float r2r = sv[8][k], r2i = sv[9][k];  // rot^2
+        const float2 R2r = f2(r2r, r2r), R2i = f2(r2i, r2i);
 #pragma unroll
-      for (int q = 0; q < K; ++q) {
-        if (q > 0) {
-          if (uniform) {  // z <- z * exp(i dw tau)
-            const float tr = zr * rr - zi * ri;
-            zi = fmaf(zr, ri, zi * rr);
-            zr = tr;
-          } else {
-            __sincosf((float)reduce_2pi(wk[q] * tau), &zi, &zr);
-          }
+        for (int pq = 1; pq < K / 2; ++pq) {
+          zr[pq] = fma2(zr[pq - 1], R2r, mul2(neg2(zi[pq - 1]), R2i));
+          zi[pq] = fma2(zr[pq - 1], R2i, mul2(zi[pq - 1], R2r));
         }
-        // e += (a + i kap b') (zr + i zi)
-        const float cx = kap[q] * bx, cy = kap[q] * by, cz = kap[q] * bz;
-        e[q][0] = fmaf(ax, zr, fmaf(-cx, zi, e[q][0])); e[q][1] = fmaf(ax, zi, fmaf(cx, zr, e[q][1]));
-        e[q][2] = fmaf(ay, zr, fmaf(-cy, zi, e[q][2])); e[q][3] = fmaf(ay, zi, fmaf(cy, zr, e[q][3]));
-        e[q][4] = fmaf(az, zr, fmaf(-cz, zi, e[q][4])); e[q][5] = fmaf(az, zi, fmaf(cz, zr, e[q][5]));
+      } else {
+        float cr[K], ci[K];
+        cr[0] = z0r;
+        ci[0] = z0i;
+#pragma unroll
+        for (int q = 1; q < K; ++q) __sincosf((float)reduce_2pi(wk[q] * tau), &ci[q], &cr[q]);
+#pragma unroll
+        for (int pq = 0; pq < K / 2; ++pq) {
+          zr[pq] = f2(cr[2 * pq], cr[2 * pq + 1]);
+          zi[pq] = f2(ci[2 * pq], ci[2 * pq + 1]);
+        }
+      }
+      const float2 Ax = f2(ax, ax), Ay = f2(ay, ay), Az = f2(az, az);
+      const float2 Bx = f2(bx, bx), By = f2(by, by), Bz = f2(bz, bz);
+#pragma unroll
+      for (int pq = 0; pq < K / 2; ++pq) {
+        // e += (a + i kap b') z, kap = -c/w per energy
+        const float2 cx = mul2(kap2[pq], Bx), cy = mul2(kap2[pq], By), cz = mul2(kap2[pq], Bz);
+        acc[pq][0] = fma2(Ax, zr[pq], fma2(neg2(cx), zi[pq], acc[pq][0]));
+        acc[pq][1] = fma2(Ax, zi[pq], fma2(cx, zr[pq], acc[pq][1]));
+        acc[pq][2] = fma2(Ay, zr[pq], fma2(neg2(cy), zi[pq], acc[pq][2]));
+        acc[pq][3] = fma2(Ay, zi[pq], fma2(cy, zr[pq], acc[pq][3]));
+        acc[pq][4] = fma2(Az, zr[pq], fma2(neg2(cz), zi[pq], acc[pq][4]));
+        acc[pq][5] = fma2(Az, zi[pq], fma2(cz, zr[pq], acc[pq][5]));
       }
     }
 #pragma unroll
-    for (int q = 0; q < K; ++q)
+    for (int pq = 0; pq < K / 2; ++pq)
 #pragma unroll
-      for (int c = 0; c < 6; ++c) E[q][c] += (double)e[q][c];
+      for (int c = 0; c < 6; ++c) {
+        E[2 * pq][c] += (double)acc[pq][c].x;
+        E[2 * pq + 1][c] += (double)acc[pq][c].y;
+      }
   }
   if (active) {
 #pragma unroll

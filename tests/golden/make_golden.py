@@ -160,6 +160,19 @@ def beam():
          flux_map=values(f), flux_map_len=len(f), pd_map=values(p), pd_map_len=len(p), draws=np.array(u))
 
 
+def beam32():
+    """Config 3a on a 32-particle subsample: 20001-point trajectories, 2000 energies over 100-1000 eV on
+    axis at 30 m, summed with weight 1/32, after set_seed(0) in a fresh process."""
+    o = new_sr()
+    W.setup_beam(o, 20001, **W.BEAM_3A)
+    W.setup_undulator(o)
+    o.set_seed(0)
+    with redirect_stdout(io.StringIO()):
+        s = np.array(o.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], npoints=2000, energy_range_eV=[100, 1000],
+                                          nparticles=32, nthreads=NT))
+    save("beam32_cfg3a.npz", energies=s[:, 0], flux=s[:, 1])
+
+
 def grid():
     """Config 4 field from an OSCARS-format grid file."""
     z, by = W.config4_grid()
@@ -255,7 +268,7 @@ def quirks():
 
 
 if __name__ == "__main__":
-    parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "grid", "adjoint", "quirks"]
+    parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "beam32", "grid", "adjoint", "quirks"]
     if "cfg0" in parts:
         e1 = cfg0()
         print("E1 (first-harmonic peak of the config-0 spectrum):", repr(e1))
@@ -263,7 +276,8 @@ if __name__ == "__main__":
             print("NOTE: update workloads.E1_EV to", repr(e1))
     if "cfg1" in parts:
         cfg1(W.E1_EV)
-    for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("grid", grid), ("adjoint", adjoint),
+    for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("beam32", beam32), ("grid", grid),
+                     ("adjoint", adjoint),
                      ("quirks", quirks)):
         if name in parts:
             fn()

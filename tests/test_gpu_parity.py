@@ -406,3 +406,22 @@ def test_spectrum_mixed_within_tolerance():
     e, f = o.spectrum_arrays([0, 0, 30], points_eV=[151.0, 152.25225225225225, 455.0, 460.1], precision="mixed")
     e2, f2 = o.spectrum_arrays([0, 0, 30], points_eV=[151.0, 152.25225225225225, 455.0, 460.1])
     assert_mixed(f, f2)
+
+
+def test_beam_spectrum_cfg3a_subsample():
+    """Config 3a at its shape (20001-point trajectories, 2000 energies over 100-1000 eV, weight
+    1/nparticles) on the reference's own 32-particle subsample from set_seed(0): plain FP64 end to end,
+    and the mixed-precision batched path against it."""
+    from srsoriginal_b200.sr import reset_random
+    g = golden("beam32_cfg3a.npz")
+    o = new_sr(20001, **W.BEAM_3A)
+    kw = dict(obs=[0, 0, W.SCREEN_Z], npoints=2000, energy_range_eV=[100, 1000], nparticles=32)
+    reset_random(0)
+    o.set_seed(0)
+    e, f64 = o.spectrum_arrays(**kw, precision="fp64")
+    assert np.array_equal(e, g["energies"])
+    assert_e2e(f64, g["flux"])
+    reset_random(0)
+    o.set_seed(0)
+    _, fm = o.spectrum_arrays(**kw, precision="mixed")
+    assert_mixed(fm, f64)
