@@ -57,18 +57,23 @@ __global__ void __launch_bounds__(kThreads) flux_mixed_kernel(const double *__re
 
 // ---------------------------------------------------------------- power density on a grid
 
-__global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
+__global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
                                                             const double *__restrict__ Ac, int64_t n, srs_grid2d g,
                                                             double nx_, double ny_, double nz_, int directional,
                                                             int64_t chunk, double *__restrict__ partial) {
   // (1 - n.beta)^5 ~ 1e-39 does not fit FP32, so the FP32 term is scaled: with omb = 1 - |beta|,
   // 1 - n.beta = omb_i * opn, opn = 1 + (|beta|/(2 omb_i)) |n - bhat|^2 >= 1, and
   // 1/(1 - n.beta)^5 = (omb_ref/omb_i)^5 / opn^5 / omb_ref^5; the last factor (~1e39) is applied in FP64.
-  // Per trajectory point i, five float4 records read as broadcasts:
-  //   r0 = (n_c, 1/D_c)                 r1 = (n_c - bhat, 1/(2 D_c))
-  //   r2 = (bhat (1 - |beta|), omb_i)   r3 = (a/c, |beta|/(2 omb_i))
-  //   r4 = (bhat . a, (omb_ref/omb_i)^5, n_c . normal, unused)
-  __shared__ float4 sm[5][kSub];
+  // Per trajectory point, 19 FP32 values anchored at the tile centre, stored for pairs of consecutive
+  // points as in the flux tile (record g of pair q = fields 2g, 2g+1 of both points):
+  //   0-2 n_c        3 1/D_c        4-6 n_c - bhat      7 1/(2 D_c)
+  //   8-10 bhat (1 - |beta|)        11 omb_i = 1 - |beta_i|
+  //   12-14 a/c      15 |beta|/(2 omb_i)                16 bhat . a/c
+  //   17 (omb_ref/omb_i)^5          18 n_c . normal     (19: padding)
+  constexpr int kPdFields = 20;
+  __shared__ float4 sm[kPdFields / 2][kSub / 2];
+  float *rec = &sm[0][0].x;
+  auto put = [&](int t, int f, float v) { rec[((f >> 1) * (kSub / 2) + (t >> 1)) * 4 + (f & 1) * 2 + (t & 1)] = v; };
   const int tid = threadIdx.x;
   const int nt2 = (g.n2 + kTileB - 1) / kTileB;
   const int T1 = blockIdx.x / nt2, T2 = blockIdx.x % nt2;
@@ -87,8 +92,10 @@ __global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__rest
   const int da = i1 - ca, db = i2 - cb;
   float Dl[3];
   for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);
-  const float dd = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
-  const float nrx = (float)nx_, nry = (float)ny_, nrz = (float)nz_;
+  const float2 Dx = f2(Dl[0], Dl[0]), Dy = f2(Dl[1], Dl[1]), Dz = f2(Dl[2], Dl[2]);
+  const float ddv = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
+  const float2 dd = f2(ddv, ddv), one = f2(1.0f, 1.0f);
+  const float2 NRx = f2((float)nx_, (float)nx_), NRy = f2((float)ny_, (float)ny_), NRz = f2((float)nz_, (float)nz_);
   double omb_ref;
   {
     const double bx = bp[0], by = bp[n], bz = bp[2 * n];
@@ -104,45 +111,66 @@ __global__ void __launch_bounds__(kThreads) pd_mixed_kernel(const double *__rest
       const Anchor A = make_anchor(Oc, xp, bp, n, i);
       const double ax = ap[i], ay = ap[n + i], az = ap[2 * n + i];
       const double r = omb_ref / A.omb;
-      sm[0][tid] = make_float4((float)A.nc[0], (float)A.nc[1], (float)A.nc[2], (float)A.invDc);
-      sm[1][tid] = make_float4((float)A.dc[0], (float)A.dc[1], (float)A.dc[2], (float)(0.5 * A.invDc));
-      sm[2][tid] = make_float4((float)(A.bhat[0] * A.omb), (float)(A.bhat[1] * A.omb), (float)(A.bhat[2] * A.omb),
-                               (float)A.omb);
-      sm[3][tid] = make_float4((float)ax, (float)ay, (float)az, (float)(0.5 * A.bmag / A.omb));
-      sm[4][tid] = make_float4((float)(A.bhat[0] * ax + A.bhat[1] * ay + A.bhat[2] * az), (float)(r * r * r * r * r),
-                               (float)(A.nc[0] * nx_ + A.nc[1] * ny_ + A.nc[2] * nz_), 0.f);
+      put(tid, 0, (float)A.nc[0]); put(tid, 1, (float)A.nc[1]); put(tid, 2, (float)A.nc[2]);
+      put(tid, 3, (float)A.invDc);
+      put(tid, 4, (float)A.dc[0]); put(tid, 5, (float)A.dc[1]); put(tid, 6, (float)A.dc[2]);
+      put(tid, 7, (float)(0.5 * A.invDc));
+      put(tid, 8, (float)(A.bhat[0] * A.omb)); put(tid, 9, (float)(A.bhat[1] * A.omb));
+      put(tid, 10, (float)(A.bhat[2] * A.omb));
+      put(tid, 11, (float)A.omb);
+      put(tid, 12, (float)ax); put(tid, 13, (float)ay); put(tid, 14, (float)az);
+      put(tid, 15, (float)(0.5 * A.bmag / A.omb));
+      put(tid, 16, (float)(A.bhat[0] * ax + A.bhat[1] * ay + A.bhat[2] * az));
+      put(tid, 17, (float)(r * r * r * r * r));
+      put(tid, 18, (float)(A.nc[0] * nx_ + A.nc[1] * ny_ + A.nc[2] * nz_));
+    } else if (tid == cnt && (cnt & 1)) {
+      // the odd count's partner slot: zero 1/D_c and (omb_ref/omb)^5 make its term 0; omb = 1 keeps
+      // 1 - n.beta finite
+      for (int f = 0; f < 19; ++f) put(tid, f, f == 11 ? 1.0f : 0.0f);
     }
     __syncthreads();
     if (!active) continue;
-    float acc = 0;
-#pragma unroll 4
-    for (int k = 0; k < cnt; ++k) {
-      const float4 r0 = sm[0][k], r1 = sm[1][k];
-      const float gq = fmaf(r0.z, Dl[2], fmaf(r0.y, Dl[1], r0.x * Dl[0]));  // n_c . Delta
-      const float h = fmaf(-gq, gq, dd);
-      const float del = fmaf(h, r1.w, gq);                                    // D_j - D_c
-      const float t = del * r0.w;
-      const float rinv = fmaf(-t, r0.w, r0.w);                                // 1/D_j
-      const float dnx = fmaf(-r0.x, del, Dl[0]) * rinv, dny = fmaf(-r0.y, del, Dl[1]) * rinv,
-                  dnz = fmaf(-r0.z, del, Dl[2]) * rinv;                       // n_j - n_c
-      const float4 r4 = sm[4][k];
-      const float nd = fmaf(dnz, nrz, fmaf(dny, nry, fmaf(dnx, nrx, r4.z)));  // n_j . normal
-      if (directional && nd <= 0.0f) continue;
-      const float4 r2 = sm[2][k], r3 = sm[3][k];
-      const float dx = r1.x + dnx, dy = r1.y + dny, dz = r1.z + dnz;           // n_j - bhat
-      const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-      const float opn = fmaf(r3.w, d2, 1.0f);  // (1 - n.beta) / omb_i
-      const float opnb = r2.w * opn;           // 1 - n.beta
-      const float na = fmaf(dz, r3.z, fmaf(dy, r3.y, fmaf(dx, r3.x, r4.x)));  // n . a
+    float2 acc = f2(0.f, 0.f);
+    const int pairs = (cnt + 1) >> 1;
+#pragma unroll 2
+    for (int q = 0; q < pairs; ++q) {
+      const float4 R0 = sm[0][q], R1 = sm[1][q], R2 = sm[2][q], R3 = sm[3][q], R4 = sm[4][q];
+      const float4 R5 = sm[5][q], R6 = sm[6][q], R7 = sm[7][q], R8 = sm[8][q], R9 = sm[9][q];
+      const float2 ncx = f2(R0.x, R0.y), ncy = f2(R0.z, R0.w), ncz = f2(R1.x, R1.y), w = f2(R1.z, R1.w);
+      const float2 dcx = f2(R2.x, R2.y), dcy = f2(R2.z, R2.w), dcz = f2(R3.x, R3.y), hinv = f2(R3.z, R3.w);
+      const float2 box = f2(R4.x, R4.y), boy = f2(R4.z, R4.w), boz = f2(R5.x, R5.y), omb = f2(R5.z, R5.w);
+      const float2 acx = f2(R6.x, R6.y), acy = f2(R6.z, R6.w), acz = f2(R7.x, R7.y), bfac = f2(R7.z, R7.w);
+      const float2 ba = f2(R8.x, R8.y), r5 = f2(R8.z, R8.w), ncn = f2(R9.x, R9.y);
+      const float2 gq = fma2(ncz, Dz, fma2(ncy, Dy, mul2(ncx, Dx)));  // n_c . Delta
+      const float2 h = fma2(neg2(gq), gq, dd);
+      const float2 del = fma2(h, hinv, gq);                          // D_j - D_c
+      const float2 t = mul2(del, w);
+      const float2 rinv = fma2(neg2(t), w, w);                       // 1/D_j
+      const float2 dnx = mul2(fma2(neg2(ncx), del, Dx), rinv);       // n_j - n_c
+      const float2 dny = mul2(fma2(neg2(ncy), del, Dy), rinv);
+      const float2 dnz = mul2(fma2(neg2(ncz), del, Dz), rinv);
+      const float2 nd = fma2(dnz, NRz, fma2(dny, NRy, fma2(dnx, NRx, ncn)));  // n_j . normal
+      const float2 dx = add2(dcx, dnx), dy = add2(dcy, dny), dz = add2(dcz, dnz);  // n_j - bhat
+      const float2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+      const float2 opn = fma2(bfac, d2, one);                        // (1 - n.beta) / omb_i
+      const float2 opnb = mul2(omb, opn);                            // 1 - n.beta
+      const float2 na = fma2(dz, acz, fma2(dy, acy, fma2(dx, acx, ba)));  // n . a
       // V = n x ((n - beta) x a) = (n - beta)(n.a) - a (1 - n.beta)
-      const float Xx = dx + r2.x, Xy = dy + r2.y, Xz = dz + r2.z;
-      const float Vx = fmaf(Xx, na, -r3.x * opnb), Vy = fmaf(Xy, na, -r3.y * opnb), Vz = fmaf(Xz, na, -r3.z * opnb);
-      const float v2 = fmaf(Vz, Vz, fmaf(Vy, Vy, Vx * Vx));
-      const float o2 = opn * opn;
-      const float o5 = o2 * o2 * opn;
-      acc = fmaf(v2 * rinv * rinv * nd * r4.y, __fdividef(1.0f, o5), acc);
+      const float2 Vx = fma2(add2(dx, box), na, mul2(neg2(acx), opnb));
+      const float2 Vy = fma2(add2(dy, boy), na, mul2(neg2(acy), opnb));
+      const float2 Vz = fma2(add2(dz, boz), na, mul2(neg2(acz), opnb));
+      const float2 v2 = fma2(Vz, Vz, fma2(Vy, Vy, mul2(Vx, Vx)));
+      const float2 o2 = mul2(opn, opn);
+      const float2 o5 = mul2(mul2(o2, o2), opn);
+      float2 term = mul2(mul2(mul2(v2, rinv), mul2(rinv, nd)), r5);
+      term = mul2(term, f2(__fdividef(1.0f, o5.x), __fdividef(1.0f, o5.y)));
+      if (directional) {  // the reference skips the terms that see the back of the surface
+        term.x = nd.x > 0.0f ? term.x : 0.0f;
+        term.y = nd.y > 0.0f ? term.y : 0.0f;
+      }
+      acc = add2(acc, term);
     }
-    sum += (double)acc;
+    sum += (double)acc.x + (double)acc.y;
   }
   const double r2 = 1.0 / (omb_ref * omb_ref);
   if (active) partial[((int64_t)p * S + s) * np + j] = sum * (r2 * r2 / omb_ref);
