@@ -171,6 +171,98 @@ def cpu_baseline(target_s=10.0):
                       f"both energies, {GRID_N} x {rows} of the 101 x 101 map ({ev:.3g} evals, {dt:.1f} s)"}
 
 
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baselines_all():
+    """The reference's CPU path (oracle/_ref, nthreads = all host threads) on every configuration,
+    each on a bounded sample scaled to the whole configuration by its evaluation count.  For the
+    record next to the GPU numbers; the bench's headline baseline is config 1 (cpu_baseline)."""
+    import io
+    from contextlib import redirect_stdout
+
+    from srsoriginal_b200 import workloads as W
+    ref_sr = reference_module()
+    th = os.cpu_count() or 1
+    out = {"cpu": _cpu_model(), "threads": th}
+
+    def timed(fn):
+        t = time.perf_counter()
+        with redirect_stdout(io.StringIO()):
+            fn()
+        return time.perf_counter() - t
+
+    def beam(npts, fields=W.setup_undulator, **kw):
+        o = ref_sr.sr()
+        W.setup_beam(o, npts, **kw)
+        fields(o)
+        return o
+
+    o = beam(NT)
+    s = timed(lambda: o.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], npoints=1000, energy_range_eV=[100, 1000],
+                                           nthreads=th))
+    out["cfg0_spectrum"] = {"evals": NT * 1000, "seconds": s, "evals_per_s": NT * 1000 / s, "sample": "whole"}
+    dt, ev = reference_sample(4, th)
+    out["cfg1_flux_maps"] = {"evals": EVALS_PER_STEP, "evals_per_s": ev / dt,
+                             "seconds_projected": EVALS_PER_STEP / (ev / dt), "sample": f"{GRID_N} x 4 rows, both maps"}
+    o = beam(40001, W.setup_epu)
+    rows = 4
+    s = timed(lambda: o.calculate_power_density_rectangle(plane="XY", width=[0.04, 0.04 * (rows - 1) / 200],
+                                                          npoints=[201, rows], translation=[0, 0, W.SCREEN_Z],
+                                                          nthreads=th))
+    ev = 40001 * 201 * rows
+    out["cfg2_power_density"] = {"evals": 40001 * 201 * 201, "evals_per_s": ev / s,
+                                 "seconds_projected": 40001 * 201 * 201 / (ev / s), "sample": f"201 x {rows} rows"}
+    o = beam(NT, **W.BEAM_3A)
+    o.set_seed(0)
+    npart = 2
+    s = timed(lambda: o.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], npoints=2000, energy_range_eV=[100, 1000],
+                                           nparticles=npart, nthreads=th))
+    ev = npart * NT * 2000
+    out["cfg3a_beam_spectrum"] = {"evals": 4096 * NT * 2000, "evals_per_s": ev / s,
+                                  "seconds_projected": 4096 * NT * 2000 / (ev / s),
+                                  "sample": f"{npart} of the 4096 particles (the reference loops over particles)"}
+    specs = W.config3b_jobs()[:16]
+    tot_ev, tot_s = 0.0, 0.0
+    for sp in specs:
+        o = beam(sp["nt"])
+        if sp["kind"] == "flux":
+            n = sp["n"]
+            tot_s += timed(lambda: o.calculate_flux_rectangle(plane="XY", energy_eV=W.E1_EV, width=[0.01, 0.01],
+                                                              npoints=[n, n], translation=[0, 0, W.SCREEN_Z],
+                                                              nthreads=th))
+            tot_ev += sp["nt"] * n * n
+        else:
+            tot_s += timed(lambda: o.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], npoints=sp["ne"],
+                                                        energy_range_eV=[100, 1000], nthreads=th))
+            tot_ev += sp["nt"] * sp["ne"]
+    all_ev = sum(j["nt"] * (j["n"] ** 2 if j["kind"] == "flux" else j["ne"]) for j in W.config3b_jobs())
+    out["cfg3b_jobs"] = {"evals": all_ev, "evals_per_s": tot_ev / tot_s, "seconds_projected": all_ev / (tot_ev / tot_s),
+                         "sample": "the first 16 of the 256 jobs"}
+    with tempfile.TemporaryDirectory() as td:
+        z, by = W.config4_grid()
+        path = os.path.join(td, "cfg4.txt")
+        W.write_oscars_grid(path, z, by)
+        o = ref_sr.sr()
+        W.setup_beam(o, NT)
+        o.add_bfield_file(ifile=path, iformat="OSCARS")
+        e0, e1 = W.config4_energy_range()
+        s = timed(lambda: o.calculate_spectrum(obs=[0, 0, W.SCREEN_Z], npoints=W.NE4, energy_range_eV=[e0, e1],
+                                               nthreads=th))
+    out["cfg4_forward"] = {"seconds": s, "note": "the reference has no gradient: central differences over the "
+                           "2007 coordinates would take 4014 of these forward runs",
+                           "fd_gradient_seconds_projected": 4014 * s}
+    return out
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
@@ -493,7 +585,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
+    ap.add_argument("--cpu-baselines", action="store_true",
+                    help="time the reference's CPU path on every configuration and exit")
     args = ap.parse_args()
+    if args.cpu_baselines:  # the reference on every configuration, host only
+        print(json.dumps(cpu_baselines_all()), flush=True)
+        return 0
     if args.impl == "reference":  # host-only: rank 0 runs the reference's CPU path, other ranks exit
         return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
     world, rank, local = dist_init()
