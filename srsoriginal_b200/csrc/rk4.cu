@@ -181,7 +181,12 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   if (stage_doubles > 0) stage_grids(sf, sp, nfields);
   const int lane = threadIdx.x & 31;
   const int gl = lane & (G - 1), gbase = lane - gl;
-  const int pp = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 / G) + lane / G;
+  // G == 32: the block's four warps all integrate the block's one particle (the same instruction
+  // stream, so the same values) and take turns storing its points (point k by warp k mod 4): the
+  // stores leave the serial chain of any one warp.  G < 32: one warp holds 32/G particles.
+  const int pp = G == 32 ? (int)blockIdx.x
+                         : (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 / G) + lane / G;
+  const int store_turn = G == 32 ? (int)(threadIdx.x >> 5) : -1;
   const bool owner = pp < nparticles;
   const int p = owner ? pp : nparticles - 1;
   const srs_particle P = particles[p];
@@ -202,10 +207,21 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   const double C = kC, qomg = P.qomg;
   const unsigned full = 0xffffffffu;
 
+  // G == 32 (one particle per block): this lane's field is held in registers across the loop, so the
+  // serial chain reloads nothing from shared memory; narrower groups, which run many particles per SM,
+  // keep it in shared memory to leave registers for occupancy
+  Prepared myp;
+  srs_field myf;
+  if (G == 32) {
+    myp = sp[fidx];
+    myf = sf[fidx];
+  }
+  const Prepared &fp = G == 32 ? myp : sp[fidx];
+  const srs_field &ff = G == 32 ? myf : sf[fidx];
   // B at two positions, one per slot, summed over fields in field order
   auto fields2 = [&](V3 pa, V3 pb, V3 &Ba, V3 &Bb) {
     V3 mine = v3(0, 0, 0);
-    if (nfields > 0) mine = field_one(sp[fidx], sf[fidx], slot == 0 ? pa : pb);
+    if (nfields > 0) mine = field_one(fp, ff, slot == 0 ? pa : pb);
     Ba = v3(0, 0, 0);
     Bb = v3(0, 0, 0);
     for (int f = 0; f < nfields; ++f) {
@@ -219,6 +235,7 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   const double rC = 1.0 / C;
   double *const my_sink = sink + (threadIdx.x & 127);
   auto store = [&](int64_t k, bool keep, V3 pos, V3 vel, V3 acc) {
+    if (store_turn >= 0 && (int)(k & 3) != store_turn) return;  // warp-uniform
 #pragma unroll
     for (int r = 0; r < (9 + G - 1) / G; ++r) {
       const int c = gl + r * G;
@@ -356,11 +373,14 @@ __global__ void field_eval_kernel(const srs_field *__restrict__ fields, int nfie
 // Lanes per particle: at least 2 * nfields (two positions per round, one field per lane), rounded
 // up to a power of two; then as many as keep the warps at <= 16 per SM, since wider groups store a
 // point's nine components in parallel and shorten the per-step chain, while narrower groups serve
-// more particles per instruction once there are enough particles to fill the SMs.
+// more particles per instruction once there are enough particles to fill the SMs.  G = 32 gives a
+// particle a whole block (four warps sharing the stores), so it is taken only while that fits.
 static int group_size(int nparticles, int nfields) {
+  constexpr int64_t kLanes = (int64_t)148 * 16 * 32;  // 16 warps per SM
   int G = 2;
   while (G < 2 * nfields) G *= 2;
-  while (G < 32 && (int64_t)nparticles * (2 * G) <= (int64_t)148 * 16 * 32) G *= 2;
+  while (G < 16 && (int64_t)nparticles * (2 * G) <= kLanes) G *= 2;
+  if (G == 16 && (int64_t)nparticles * 4 * 32 <= kLanes) G = 32;
   return G;
 }
 
@@ -388,7 +408,7 @@ static cudaError_t launch_warp_rk4_g(const srs_field *d_fields, int nfields, con
                               const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s) {
   const size_t smem = sizeof(double) * (size_t)stage_doubles;
   if (cudaError_t e = allow_smem(rk4_warp_kernel<G>, smem)) return e;
-  const int warps = 4, per_block = warps * (32 / G);
+  const int warps = 4, per_block = G == 32 ? 1 : warps * (32 / G);
   rk4_warp_kernel<G><<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
       d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, d_specs, stage_doubles);
   return cudaGetLastError();
