@@ -337,6 +337,15 @@ def measure_configs(dev):
     out["cfg0_spectrum"] = {"evals": ev, "fp64_ms": ms, "fp64_evals_per_s": ev / (ms * 1e-3), "mixed_ms": msm,
                             "mixed_evals_per_s": ev / (msm * 1e-3)}
 
+    # config 1's first map as a plain point list (no grid to anchor on): the point-list mixed kernel
+    xyz1, _, _, _ = rectangle_points([GRID_N, GRID_N], "XY", [WIDTH, WIDTH], translation=[0, 0, W.SCREEN_Z])
+    pts1 = torch.as_tensor(np.ascontiguousarray(xyz1.reshape(-1)), device=dev)
+    fl = torch.empty(GRID_N * GRID_N, dtype=torch.float64, device=dev)
+    msp = _events_ms(lambda: D.flux(traj, charge, current, E1, fl, points=pts1, precision=_lib.MIXED), 5)
+    ev = NT * GRID_N * GRID_N
+    out["cfg1_map_as_point_list"] = {"evals": ev, "mixed_ms": msp, "mixed_evals_per_s": ev / (msp * 1e-3),
+                                     "kernel": "FP64 geometry and phase per term, FP32 amplitude (no grid anchor)"}
+
     # config 2: power density of the elliptical undulator, 201 x 201 on a 40 mm square, 40001 points
     epu = [D.undulator([0, 1.0, 0], [0, 0, W.PERIOD], W.NPERIODS),
            D.undulator([0.6, 0, 0], [0, 0, W.PERIOD], W.NPERIODS, phase=np.pi / 2)]

@@ -138,8 +138,10 @@ srs_status srs_spectrum(srs_traj_view traj, srs_beam_consts beam, const double o
 
 /* Flux at np observation points at one photon energy (OSCARSSR_Cuda_CalculateFluxGPU /
  * OSCARSSR.cc:1989-2099).  d_points: DEVICE, 3*np doubles (x,y,z per point).  d_out: DEVICE,
- * nparticles*np values.  For SRS_PRECISION_MIXED the points must form a regular grid given by grid
- * (see srs_grid2d) and d_points may be NULL. */
+ * nparticles*np values.  For SRS_PRECISION_MIXED, points that form a regular grid are best given as
+ * grid (see srs_grid2d; d_points may then be NULL): the tiles anchor the FP64 geometry on it.  With
+ * grid NULL any list of points is accepted; the geometry and phase are then FP64 per term and the
+ * amplitude, sincos and accumulation FP32. */
 typedef struct srs_grid2d {
   double origin[3]; /* point (0,0) */
   double u1[3];     /* step to point (1,0) */
@@ -171,8 +173,9 @@ srs_status srs_flux_mixed_noalloc(srs_traj_view traj, srs_beam_consts beam, cons
 /* Power density at np points with unit normals (OSCARSSR.cc:1477-1598; the reference's CPU
  * semantics: with directional != 0 the terms with n.normal <= 0 are skipped, otherwise the result is
  * made non-negative).  d_points, d_normals: DEVICE 3*np doubles.  d_out: DEVICE nparticles*np values
- * in W/mm^2 (weight 1).  For SRS_PRECISION_MIXED the points must form the regular grid `grid`
- * (normal included) and d_points/d_normals may be NULL. */
+ * in W/mm^2 (weight 1).  For SRS_PRECISION_MIXED a regular grid with one normal is best given as
+ * `grid` (d_points/d_normals may then be NULL); with grid NULL any points with their own normals are
+ * accepted (FP64 geometry per term, FP32 for the rest). */
 srs_status srs_power_density(srs_traj_view traj, srs_beam_consts beam, const double *d_points,
                              const double *d_normals, int64_t np, const srs_grid2d *grid,
                              int32_t directional, int32_t precision, double *d_out, void *stream);

@@ -127,11 +127,16 @@ srs_status srs_flux(srs_traj_view traj, srs_beam_consts beam, const double *d_po
     SRS_CUDA(scratch.alloc(fp64_flux_scratch_bytes(traj.n, np, traj.nparticles), s));
     SRS_CUDA(fp64_flux(traj, beam, d_points, np, energy_ev, d_out, scratch.ptr, s));
   } else if (precision == SRS_PRECISION_MIXED) {
-    if (!grid) return fail(SRS_ERR_INVALID, "mixed-precision flux needs the points as a regular grid");
-    if ((int64_t)grid->n1 * grid->n2 != np || grid->n1 < 1 || grid->n2 < 1)
-      return fail(SRS_ERR_INVALID, "grid size does not match the number of points");
-    SRS_CUDA(scratch.alloc(mixed_flux_scratch_bytes(traj.n, *grid, traj.nparticles), s));
-    SRS_CUDA(mixed_flux(traj, beam, *grid, energy_ev, d_out, scratch.ptr, s));
+    if (grid) {  // a regular grid: the tiles anchor on it
+      if ((int64_t)grid->n1 * grid->n2 != np || grid->n1 < 1 || grid->n2 < 1)
+        return fail(SRS_ERR_INVALID, "grid size does not match the number of points");
+      SRS_CUDA(scratch.alloc(mixed_flux_scratch_bytes(traj.n, *grid, traj.nparticles), s));
+      SRS_CUDA(mixed_flux(traj, beam, *grid, energy_ev, d_out, scratch.ptr, s));
+    } else {  // any list of points
+      if (!d_points) return fail(SRS_ERR_INVALID, "NULL points");
+      SRS_CUDA(scratch.alloc(mixed_flux_points_scratch_bytes(traj.n, np, traj.nparticles), s));
+      SRS_CUDA(mixed_flux_points(traj, beam, d_points, np, energy_ev, d_out, scratch.ptr, s));
+    }
   } else {
     return fail(SRS_ERR_INVALID, "unknown precision");
   }
@@ -152,11 +157,16 @@ srs_status srs_power_density(srs_traj_view traj, srs_beam_consts beam, const dou
     SRS_CUDA(scratch.alloc(fp64_pd_scratch_bytes(traj.n, np, traj.nparticles), s));
     SRS_CUDA(fp64_power_density(traj, beam, d_points, d_normals, np, directional, d_out, scratch.ptr, s));
   } else if (precision == SRS_PRECISION_MIXED) {
-    if (!grid) return fail(SRS_ERR_INVALID, "mixed-precision power density needs the points as a regular grid");
-    if ((int64_t)grid->n1 * grid->n2 != np || grid->n1 < 1 || grid->n2 < 1)
-      return fail(SRS_ERR_INVALID, "grid size does not match the number of points");
-    SRS_CUDA(scratch.alloc(mixed_pd_scratch_bytes(traj.n, *grid, traj.nparticles), s));
-    SRS_CUDA(mixed_power_density(traj, beam, *grid, directional, d_out, scratch.ptr, s));
+    if (grid) {  // a regular grid (one normal): the tiles anchor on it
+      if ((int64_t)grid->n1 * grid->n2 != np || grid->n1 < 1 || grid->n2 < 1)
+        return fail(SRS_ERR_INVALID, "grid size does not match the number of points");
+      SRS_CUDA(scratch.alloc(mixed_pd_scratch_bytes(traj.n, *grid, traj.nparticles), s));
+      SRS_CUDA(mixed_power_density(traj, beam, *grid, directional, d_out, scratch.ptr, s));
+    } else {  // any points, each with its own normal
+      if (!d_points || !d_normals) return fail(SRS_ERR_INVALID, "NULL points or normals");
+      SRS_CUDA(scratch.alloc(mixed_pd_points_scratch_bytes(traj.n, np, traj.nparticles), s));
+      SRS_CUDA(mixed_power_density_points(traj, beam, d_points, d_normals, np, directional, d_out, scratch.ptr, s));
+    }
   } else {
     return fail(SRS_ERR_INVALID, "unknown precision");
   }

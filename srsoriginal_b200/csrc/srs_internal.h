@@ -91,6 +91,14 @@ cudaError_t mixed_spectrum(const srs_traj_view &t, const srs_beam_consts &b, con
 size_t mixed_flux_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles);
 cudaError_t mixed_flux(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g, double energy_ev,
                        double *d_out, void *scratch, cudaStream_t s);
+// Mixed-precision flux at an arbitrary list of points (FP64 geometry and phase, FP32 amplitude).
+size_t mixed_flux_points_scratch_bytes(int64_t n, int64_t np, int nparticles);
+cudaError_t mixed_flux_points(const srs_traj_view &t, const srs_beam_consts &b, const double *d_points, int64_t np,
+                              double energy_ev, double *d_out, void *scratch, cudaStream_t s);
+size_t mixed_pd_points_scratch_bytes(int64_t n, int64_t np, int nparticles);
+cudaError_t mixed_power_density_points(const srs_traj_view &t, const srs_beam_consts &b, const double *d_points,
+                                       const double *d_normals, int64_t np, int directional, double *d_out,
+                                       void *scratch, cudaStream_t s);
 size_t mixed_pd_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles);
 cudaError_t mixed_power_density(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g,
                                 int directional, double *d_out, void *scratch, cudaStream_t s);

@@ -55,6 +55,20 @@ __global__ void __launch_bounds__(kThreads) flux_mixed_kernel(const double *__re
                    blockIdx.x % nt2, i0, imin64(n, i0 + chunk), partial + ((int64_t)p * S + s) * 6 * np, sh);
 }
 
+// ---------------------------------------------------------------- flux at a list of points
+
+__global__ void __launch_bounds__(kThreads) flux_points_mixed_kernel(const double *__restrict__ X,
+                                                                     const double *__restrict__ Bt, int64_t n,
+                                                                     double dt, const double *__restrict__ points,
+                                                                     int64_t np, double omega, int64_t chunk,
+                                                                     double *__restrict__ partial) {
+  __shared__ tiles::PointsShared sh;
+  const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
+  const int64_t i0 = (int64_t)s * chunk;
+  tiles::points_flux_tile(X + (int64_t)p * 3 * n, Bt + (int64_t)p * 3 * n, n, dt, points, np, omega, blockIdx.x, i0,
+                          imin64(n, i0 + chunk), partial + ((int64_t)p * S + s) * 6 * np, sh);
+}
+
 // ---------------------------------------------------------------- power density on a grid
 
 __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
@@ -176,6 +190,93 @@ __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__r
   if (active) partial[((int64_t)p * S + s) * np + j] = sum * (r2 * r2 / omb_ref);
 }
 
+// ---------------------------------------------------------------- power density at a list of points
+
+// Each thread one observation point with its own normal; FP64 geometry per (point, trajectory point)
+// -- R, |R| (FP32 reciprocal square root refined by two Newton steps), n and n - bhat -- and the
+// rest in FP32 with the grid kernel's scaling of (1 - n.beta)^-5.
+__global__ void __launch_bounds__(kThreads) pd_points_mixed_kernel(const double *__restrict__ X,
+                                                                   const double *__restrict__ Bt,
+                                                                   const double *__restrict__ Ac, int64_t n,
+                                                                   const double *__restrict__ points,
+                                                                   const double *__restrict__ normals, int64_t np,
+                                                                   int directional, int64_t chunk,
+                                                                   double *__restrict__ partial) {
+  __shared__ double sx[3][kSub], sbh[3][kSub];
+  __shared__ float sf[10][kSub];  // bhat omb (3), omb, a/c (3), |beta|/(2 omb), bhat.a, (omb_ref/omb)^5
+  const int tid = threadIdx.x;
+  const int64_t j = (int64_t)blockIdx.x * kThreads + tid;
+  const bool active = j < np;
+  const int64_t jj = active ? j : np - 1;
+  const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
+  const int64_t off = (int64_t)p * 3 * n;
+  const double *xp = X + off, *bp = Bt + off, *ap = Ac + off;
+  const int64_t i0 = (int64_t)s * chunk, iend = imin64(n, i0 + chunk);
+  const double Px = points[3 * jj], Py = points[3 * jj + 1], Pz = points[3 * jj + 2];
+  const float nrx = (float)normals[3 * jj], nry = (float)normals[3 * jj + 1], nrz = (float)normals[3 * jj + 2];
+  double omb_ref;
+  {
+    const double bx = bp[0], by = bp[n], bz = bp[2 * n];
+    const double b2 = bx * bx + by * by + bz * bz;
+    omb_ref = (1.0 - b2) / (1.0 + sqrt(b2));
+  }
+  double sum = 0;
+  for (int64_t base = i0; base < iend; base += kSub) {
+    const int cnt = (int)imin64(kSub, iend - base);
+    __syncthreads();
+    if (tid < cnt) {
+      const int64_t i = base + tid;
+      const double bx = bp[i], by = bp[n + i], bz = bp[2 * n + i];
+      const double b2 = bx * bx + by * by + bz * bz, bm = sqrt(b2), ib = 1.0 / bm;
+      const double omb = (1.0 - b2) / (1.0 + bm);
+      const double hx = bx * ib, hy = by * ib, hz = bz * ib;
+      const double ax = ap[i], ay = ap[n + i], az = ap[2 * n + i];
+      const double r = omb_ref / omb;
+      sx[0][tid] = xp[i]; sx[1][tid] = xp[n + i]; sx[2][tid] = xp[2 * n + i];
+      sbh[0][tid] = hx; sbh[1][tid] = hy; sbh[2][tid] = hz;
+      sf[0][tid] = (float)(hx * omb); sf[1][tid] = (float)(hy * omb); sf[2][tid] = (float)(hz * omb);
+      sf[3][tid] = (float)omb;
+      sf[4][tid] = (float)ax; sf[5][tid] = (float)ay; sf[6][tid] = (float)az;
+      sf[7][tid] = (float)(0.5 * bm / omb);
+      sf[8][tid] = (float)(hx * ax + hy * ay + hz * az);
+      sf[9][tid] = (float)(r * r * r * r * r);
+    }
+    __syncthreads();
+    if (!active) continue;
+    float acc = 0.f;
+#pragma unroll 2
+    for (int k = 0; k < cnt; ++k) {
+      const double Rx = Px - sx[0][k], Ry = Py - sx[1][k], Rz = Pz - sx[2][k];
+      const double R2 = fma(Rx, Rx, fma(Ry, Ry, Rz * Rz));
+      const float yf = rsqrtf((float)R2);
+      double y = (double)yf;
+      double e = fma(-R2 * y, y, 1.0);
+      y = fma(0.5 * y, e, y);
+      e = fma(-R2 * y, y, 1.0);
+      y = fma(0.5 * y, e, y);  // 1/|R| to FP64 accuracy
+      const double nx = Rx * y, ny = Ry * y, nz = Rz * y;
+      const float dx = (float)(nx - sbh[0][k]), dy = (float)(ny - sbh[1][k]), dz = (float)(nz - sbh[2][k]);  // n - bhat
+      const float nd = fmaf((float)nz, nrz, fmaf((float)ny, nry, (float)nx * nrx));                           // n . normal
+      const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      const float opn = fmaf(sf[7][k], d2, 1.0f);  // (1 - n.beta) / omb_i
+      const float opnb = sf[3][k] * opn;           // 1 - n.beta
+      const float acx = sf[4][k], acy = sf[5][k], acz = sf[6][k];
+      const float na = fmaf(dz, acz, fmaf(dy, acy, fmaf(dx, acx, sf[8][k])));  // n . a
+      // V = n x ((n - beta) x a) = (n - beta)(n.a) - a (1 - n.beta)
+      const float Vx = fmaf(dx + sf[0][k], na, -acx * opnb), Vy = fmaf(dy + sf[1][k], na, -acy * opnb),
+                  Vz = fmaf(dz + sf[2][k], na, -acz * opnb);
+      const float v2 = fmaf(Vz, Vz, fmaf(Vy, Vy, Vx * Vx));
+      const float o2 = opn * opn, o5 = o2 * o2 * opn;
+      float term = v2 * (yf * yf) * nd * sf[9][k] * __fdividef(1.0f, o5);
+      if (directional && !(nd > 0.0f)) term = 0.0f;  // the reference skips the terms that see the back
+      acc += term;
+    }
+    sum += (double)acc;
+  }
+  const double r2 = 1.0 / (omb_ref * omb_ref);
+  if (active) partial[((int64_t)p * S + s) * np + j] = sum * (r2 * r2 / omb_ref);
+}
+
 // ---------------------------------------------------------------- spectrum at one observer
 
 __global__ void __launch_bounds__(kThreads) spectrum_mixed_kernel(const double *__restrict__ X,
@@ -225,6 +326,28 @@ static cudaError_t mixed_flux_splits(const srs_traj_view &t, const srs_beam_cons
 cudaError_t mixed_flux(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g, double energy_ev,
                        double *d_out, void *scratch, cudaStream_t s) {
   return mixed_flux_splits(t, b, g, energy_ev, d_out, scratch, flux_mixed_splits(t.n, g, t.nparticles), s);
+}
+
+static int flux_points_splits(int64_t n, int64_t np, int nparticles) {
+  return splits_for((np + kThreads - 1) / kThreads * nparticles, n, 256, wave_slots(flux_points_mixed_kernel));
+}
+
+size_t mixed_flux_points_scratch_bytes(int64_t n, int64_t np, int nparticles) {
+  return sizeof(double) * 6 * (size_t)np * nparticles * flux_points_splits(n, np, nparticles);
+}
+
+cudaError_t mixed_flux_points(const srs_traj_view &t, const srs_beam_consts &b, const double *d_points, int64_t np,
+                              double energy_ev, double *d_out, void *scratch, cudaStream_t s) {
+  const int64_t chunk = aligned_chunk(t.n, flux_points_splits(t.n, np, t.nparticles));
+  const int S = used_chunks(t.n, chunk);
+  const double omega = ev_to_omega(energy_ev);
+  double *partial = static_cast<double *>(scratch);
+  dim3 grid((unsigned)((np + kThreads - 1) / kThreads), S, t.nparticles);
+  flux_points_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt, d_points, np, omega, chunk, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return finish_flux_partials(partial, S, np, t.nparticles, nullptr, omega, t.dt, flux_c0(b.charge),
+                              flux_c2(b.charge, b.current), d_out, s);
 }
 
 // ---------------------------------------------------------------- allocation-free flux entry point
@@ -312,6 +435,28 @@ cudaError_t mixed_power_density(const srs_traj_view &t, const srs_beam_consts &b
   if (e != cudaSuccess) return e;
   return finish_pd_partials(partial, S, (int64_t)g.n1 * g.n2, t.nparticles, pd_const(b.charge, b.current) * t.dt,
                             directional, d_out, s);
+}
+
+static int pd_points_splits(int64_t n, int64_t np, int nparticles) {
+  return splits_for((np + kThreads - 1) / kThreads * nparticles, n, 256, wave_slots(pd_points_mixed_kernel));
+}
+
+size_t mixed_pd_points_scratch_bytes(int64_t n, int64_t np, int nparticles) {
+  return sizeof(double) * (size_t)np * nparticles * pd_points_splits(n, np, nparticles);
+}
+
+cudaError_t mixed_power_density_points(const srs_traj_view &t, const srs_beam_consts &b, const double *d_points,
+                                       const double *d_normals, int64_t np, int directional, double *d_out,
+                                       void *scratch, cudaStream_t s) {
+  const int64_t chunk = aligned_chunk(t.n, pd_points_splits(t.n, np, t.nparticles));
+  const int S = used_chunks(t.n, chunk);
+  double *partial = static_cast<double *>(scratch);
+  dim3 grid((unsigned)((np + kThreads - 1) / kThreads), S, t.nparticles);
+  pd_points_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.aoc, t.n, d_points, d_normals, np, directional,
+                                                   chunk, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return finish_pd_partials(partial, S, np, t.nparticles, pd_const(b.charge, b.current) * t.dt, directional, d_out, s);
 }
 
 size_t mixed_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles) {

@@ -389,6 +389,101 @@ class sr:  # noqa: N801  (the reference's type name)
                 else:
                     f.write(f"{c[0]:.6e} {c[1]:.6e} {c[2]:.6e} {v:.6e}\n")
 
+    # ------------------------------------------------------------ arbitrary point surfaces
+    @staticmethod
+    def _rotate_xyz(v, r):
+        """TVector3D::RotateSelfXYZ (TVector3D.cc:150-205): about X, then Y, then Z."""
+        x, y, z = v
+        s, c = math.sin(r[0]), math.cos(r[0])
+        y, z = c * y - s * z, s * y + c * z
+        s, c = math.sin(r[1]), math.cos(r[1])
+        z, x = c * z - s * x, s * z + c * x
+        s, c = math.sin(r[2]), math.cos(r[2])
+        x, y = c * x - s * y, s * x + c * y
+        return [x, y, z]
+
+    @staticmethod
+    def _surface_3d(points, rotations, translation, invert_normal):
+        """TSurfacePoints_3D from [[x, y, z], [nx, ny, nz]] pairs as the reference's point-list calls
+        build it (OSCARSSR_Python.cc:2449-2502, 2875-2920): point and normal rotated, the normal
+        optionally inverted and made a unit vector (TSurfacePoint.cc:12-16), the point translated.
+        Returns (points (N,3), unit normals (N,3))."""
+        rot = _list3(rotations, "rotations") if rotations is not None and len(rotations) != 0 else [0.0, 0.0, 0.0]
+        tr = _list3(translation, "translation") if translation is not None and len(translation) != 0 \
+            else [0.0, 0.0, 0.0]
+        xs, ns = [], []
+        for item in points:
+            if not hasattr(item, "__len__") or len(item) != 2:
+                raise ValueError("Incorrect format in 'points'")
+            try:
+                X = _list3(item[0], "points")
+                N = _list3(item[1], "points")
+            except ValueError:
+                raise ValueError("Incorrect format in 'points': Point or Normal does not have 3 elements") from None
+            X = sr._rotate_xyz(X, rot)
+            N = sr._rotate_xyz(N, rot)
+            if invert_normal:
+                N = [-N[0], -N[1], -N[2]]
+            m = math.sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2])  # TSurfacePoint keeps the unit normal
+            xs.append([X[0] + tr[0], X[1] + tr[1], X[2] + tr[2]])
+            ns.append([N[0] / m, N[1] / m, N[2] / m])
+        return np.array(xs, dtype=np.float64).reshape(-1, 3), np.array(ns, dtype=np.float64).reshape(-1, 3)
+
+    def _point_list(self, xyz, out, nparticles, nthreads, gpu, pd):
+        """The reference's list for a point surface (dim = 3): the points, then the zero entries its
+        dispatch path appends (see calculate_flux_rectangle / calculate_power_density_rectangle)."""
+        nth = nthreads if nthreads >= 1 else self._nthreads_global
+        calls = max(1, int(nparticles))
+        extra = gpu == 1 or (nth != 1 if pd else nth == 1)
+        coords = np.concatenate([xyz] + ([xyz] * calls if extra else []))
+        vals = np.concatenate([out] + ([np.zeros(len(xyz))] * calls if extra else []))
+        return coords, vals
+
+    def calculate_flux(self, energy_eV, points, normal=0, rotations=None, translation=None, nparticles=0,
+                       nthreads=0, gpu=0, ofile="", precision=None):
+        """[[[x, y, z], flux], ...] at any list of points [[x, y, z], [nx, ny, nz]]
+        (OSCARSSR_Python.cc:2829-3008; the normals are carried but unused by the flux)."""
+        if lib.srs_sim_get_nparticle_beams(self._h) < 1:
+            raise ValueError("No particle beam defined")
+        xyz, _ = self._surface_3d(points, rotations, translation, False)
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        self._check_gpu_threads(gpu, nthreads)
+        npts = len(xyz)
+        out, comp = np.zeros(npts), np.zeros(npts)
+        if npts:
+            pts = np.ascontiguousarray(xyz.reshape(-1))
+            check(lib.srs_sim_calculate_flux(self._h, dptr(pts), npts, None, float(energy_eV), int(nparticles),
+                                             self._prec(precision), dptr(out), dptr(comp)))
+        C_, V = self._point_list(xyz, out, nparticles, nthreads, gpu, pd=False)
+        if ofile:
+            self._write_points(ofile, C_, V, 3)
+        return [[c, float(v)] for c, v in zip(C_.tolist(), V)]
+
+    def calculate_power_density(self, points, normal=0, rotations=None, translation=None, nparticles=0, gpu=0,
+                                nthreads=0, ofile="", precision=None):
+        """[[[x, y, z], W/mm^2], ...] at any list of points with their normals [[x, y, z], [nx, ny, nz]]
+        (OSCARSSR_Python.cc:2403-2577): normal = -1 inverts the normals, normal != 0 makes the
+        calculation directional."""
+        if lib.srs_sim_get_nparticle_beams(self._h) < 1:
+            raise ValueError("No particle beam defined")
+        xyz, nrm = self._surface_3d(points, rotations, translation, normal == -1)
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        self._check_gpu_threads(gpu, nthreads)
+        npts = len(xyz)
+        out, comp = np.zeros(npts), np.zeros(npts)
+        if npts:
+            pts = np.ascontiguousarray(xyz.reshape(-1))
+            nrms = np.ascontiguousarray(nrm.reshape(-1))
+            check(lib.srs_sim_calculate_power_density(self._h, dptr(pts), dptr(nrms), npts, None,
+                                                      0 if normal == 0 else 1, int(nparticles), 1 if gpu == 1 else 0,
+                                                      self._prec(precision), dptr(out), dptr(comp)))
+        C_, V = self._point_list(xyz, out, nparticles, nthreads, gpu, pd=True)
+        if ofile:
+            self._write_points(ofile, C_, V, 3)
+        return [[c, float(v)] for c, v in zip(C_.tolist(), V)]
+
     # ------------------------------------------------------------ flux
     def calculate_flux_rectangle(self, energy_eV, npoints, plane="", normal=0, dim=2, width=None, rotations=None,
                                  translation=None, x0x1x2=None, nparticles=0, polarization="", nthreads=0, gpu=0,

@@ -160,6 +160,33 @@ def beam():
          flux_map=values(f), flux_map_len=len(f), pd_map=values(p), pd_map_len=len(p), draws=np.array(u))
 
 
+def points_surface():
+    """Config-0 beam on a 2001-point trajectory; 40 scattered points on a tilted patch near the axis at
+    30 m, with their own normals, through calculate_flux and calculate_power_density with rotations,
+    translation and each normal option, on the one-thread and the threaded paths."""
+    rng = np.random.default_rng(5)
+    pts = []
+    for _ in range(40):
+        x, y = rng.uniform(-0.004, 0.004, 2)
+        n = [rng.uniform(-0.2, 0.2), rng.uniform(-0.2, 0.2), 1.0]
+        pts.append([[float(x), float(y), float(30.0 + 0.2 * x)], [float(v) for v in n]])
+    o = new_sr()
+    W.setup_beam(o, 2001)
+    W.setup_undulator(o)
+    kw = dict(rotations=[2e-5, -3e-5, 0.3], translation=[0.0005, -0.0002, 0.1])
+    with redirect_stdout(io.StringIO()):
+        f1 = o.calculate_flux(energy_eV=W.E1_EV, points=pts, nthreads=1, **kw)
+        f2 = o.calculate_flux(energy_eV=W.E1_EV, points=pts, nthreads=2, **kw)
+        pd = {}
+        for nrm in (0, 1, -1):
+            pd[nrm] = o.calculate_power_density(points=pts, normal=nrm, nthreads=1, **kw)
+        pd2 = o.calculate_power_density(points=pts, normal=0, nthreads=2, **kw)
+    save("points_surface.npz", points=np.array(pts, dtype=np.float64),
+         flux_coords=coords(f1), flux=values(f1), flux_len_t1=len(f1), flux_len_t2=len(f2),
+         pd0_coords=coords(pd[0]), pd0=values(pd[0]), pd1=values(pd[1]), pdm1=values(pd[-1]),
+         pd_len_t1=len(pd[0]), pd_len_t2=len(pd2))
+
+
 def beam32():
     """Config 3a on a 32-particle subsample: 20001-point trajectories, 2000 energies over 100-1000 eV on
     axis at 30 m, summed with weight 1/32, after set_seed(0) in a fresh process."""
@@ -268,7 +295,8 @@ def quirks():
 
 
 if __name__ == "__main__":
-    parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "beam32", "grid", "adjoint", "quirks"]
+    parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "beam32", "points", "grid", "adjoint",
+                             "quirks"]
     if "cfg0" in parts:
         e1 = cfg0()
         print("E1 (first-harmonic peak of the config-0 spectrum):", repr(e1))
@@ -276,7 +304,8 @@ if __name__ == "__main__":
             print("NOTE: update workloads.E1_EV to", repr(e1))
     if "cfg1" in parts:
         cfg1(W.E1_EV)
-    for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("beam32", beam32), ("grid", grid),
+    for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("beam32", beam32), ("points", points_surface),
+                     ("grid", grid),
                      ("adjoint", adjoint),
                      ("quirks", quirks)):
         if name in parts:

@@ -353,11 +353,16 @@ def test_c_abi_rejects_bad_arguments():
     with pytest.raises(ValueError):
         _lib.check(_lib.lib.srs_spectrum(view, _lib.BeamConsts(-1.6e-19, 0.5), _lib.v3([0, 0, 1]), None, 0,
                                          _lib.FP64, None, None))
-    with pytest.raises(ValueError, match="grid"):
-        t = _dev(np.zeros(30))
-        v = _lib.TrajView(C.cast(t.data_ptr(), _lib._D), C.cast(t.data_ptr(), _lib._D),
-                          C.cast(t.data_ptr(), _lib._D), 10, 1, 1e-12)
-        _lib.check(_lib.lib.srs_flux(v, _lib.BeamConsts(-1.6e-19, 0.5), _vp(t), 3, None, 100.0, _lib.MIXED,
+    t = _dev(np.zeros(30))
+    v = _lib.TrajView(C.cast(t.data_ptr(), _lib._D), C.cast(t.data_ptr(), _lib._D),
+                      C.cast(t.data_ptr(), _lib._D), 10, 1, 1e-12)
+    with pytest.raises(ValueError, match="NULL points"):  # mixed without a grid needs the point list
+        _lib.check(_lib.lib.srs_flux(v, _lib.BeamConsts(-1.6e-19, 0.5), None, 3, None, 100.0, _lib.MIXED,
+                                     _vp(t), None))
+    g = _lib.Grid2D()
+    g.n1, g.n2 = 2, 2
+    with pytest.raises(ValueError, match="grid size"):
+        _lib.check(_lib.lib.srs_flux(v, _lib.BeamConsts(-1.6e-19, 0.5), None, 3, C.byref(g), 100.0, _lib.MIXED,
                                      _vp(t), None))
 
 
@@ -425,3 +430,63 @@ def test_beam_spectrum_cfg3a_subsample():
     o.set_seed(0)
     _, fm = o.spectrum_arrays(**kw, precision="mixed")
     assert_mixed(fm, f64)
+
+
+def test_point_surfaces_fp64_and_mixed():
+    """calculate_flux / calculate_power_density on a list of points with their own normals
+    (OSCARSSR_Python.cc:2403-2577, 2829-3008): coordinates after rotation and translation, list
+    lengths per dispatch path and values against the reference; the mixed-precision point-list
+    kernels against the plain FP64 ones."""
+    g = golden("points_surface.npz")
+    pts = g["points"].tolist()
+    o = new_sr(2001)
+    kw = dict(rotations=[2e-5, -3e-5, 0.3], translation=[0.0005, -0.0002, 0.1])
+    n = len(pts)
+    f1 = o.calculate_flux(energy_eV=W.E1_EV, points=pts, nthreads=1, **kw)
+    assert len(f1) == int(g["flux_len_t1"])
+    assert np.array_equal(np.array([c for c, _ in f1]), g["flux_coords"])
+    v1 = np.array([v for _, v in f1])
+    assert_e2e(v1[:n], g["flux"][:n])
+    assert np.all(v1[n:] == 0)
+    assert len(o.calculate_flux(energy_eV=W.E1_EV, points=pts, nthreads=2, **kw)) == int(g["flux_len_t2"])
+    assert len(o.calculate_flux(energy_eV=W.E1_EV, points=pts, gpu=1, **kw)) == 2 * n
+    fm = o.calculate_flux(energy_eV=W.E1_EV, points=pts, nthreads=1, precision="mixed", **kw)
+    assert_mixed([v for _, v in fm][:n], v1[:n])
+    for nrm, key in ((0, "pd0"), (1, "pd1"), (-1, "pdm1")):
+        p = o.calculate_power_density(points=pts, normal=nrm, nthreads=1, **kw)
+        assert len(p) == int(g["pd_len_t1"])
+        vals = np.array([v for _, v in p])
+        assert_e2e(vals, g[key])
+        if nrm == 0:
+            assert np.array_equal(np.array([c for c, _ in p]), g["pd0_coords"])
+        pm = o.calculate_power_density(points=pts, normal=nrm, nthreads=1, precision="mixed", **kw)
+        assert_mixed([v for _, v in pm], vals)
+    assert len(o.calculate_power_density(points=pts, normal=0, nthreads=2, **kw)) == int(g["pd_len_t2"])
+
+
+def test_mixed_point_list_kernels_match_grid_kernels():
+    """The point-list mixed kernels on the config-1 and config-2 grids given as plain point lists,
+    against the grid (anchored) mixed kernels and the plain FP64 kernels."""
+    import torch
+    from srsoriginal_b200 import _lib, device as D
+    from srsoriginal_b200.sr import rectangle_points
+    tr = reference_trajectory_on_device(20001)
+    xyz, _, nrm, grid = rectangle_points([101, 101], "XY", [0.01, 0.01], translation=[0, 0, 30])
+    pts = torch.as_tensor(np.ascontiguousarray(xyz.reshape(-1)), device="cuda")
+    for e in (W.E1_EV, W.E3_EV):
+        a, b, c = (torch.empty(101 * 101, dtype=torch.float64, device="cuda") for _ in range(3))
+        D.flux(tr, -O.QE, 0.5, e, a, points=pts, precision=_lib.MIXED)
+        D.flux(tr, -O.QE, 0.5, e, b, grid=grid, precision=_lib.MIXED)
+        D.flux(tr, -O.QE, 0.5, e, c, points=pts, precision=_lib.FP64)
+        torch.cuda.synchronize()
+        assert_mixed(a.cpu().numpy(), c.cpu().numpy())
+        assert_mixed(a.cpu().numpy(), b.cpu().numpy())
+    t2 = reference_trajectory_on_device(40001, "epu")
+    xyz, _, nrm, grid = rectangle_points([51, 51], "XY", [0.04, 0.04], translation=[0, 0, 30])
+    pts = torch.as_tensor(np.ascontiguousarray(xyz.reshape(-1)), device="cuda")
+    nrms = torch.as_tensor(np.ascontiguousarray(np.tile(nrm, (51 * 51, 1)).reshape(-1)), device="cuda")
+    a, c = (torch.empty(51 * 51, dtype=torch.float64, device="cuda") for _ in range(2))
+    D.power_density(t2, -O.QE, 0.5, a, points=pts, normals=nrms, precision=_lib.MIXED)
+    D.power_density(t2, -O.QE, 0.5, c, points=pts, normals=nrms, precision=_lib.FP64)
+    torch.cuda.synchronize()
+    assert_mixed(a.cpu().numpy(), c.cpu().numpy())

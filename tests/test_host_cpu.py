@@ -136,3 +136,17 @@ def test_particle_from_ic_jacobian():
         # rounding is ~1e-16 / 3e-8 relative: the differences carry that noise over 2h
         tol[6] += 1e-8 * abs(vec(ic)[6]) / h
         assert np.all(np.abs(fd - J[:, j]) <= tol), (j, fd, J[:, j])
+
+
+def test_point_surface_coordinates_match_reference():
+    """The point-list surface (rotation about X, Y, Z, normal inversion, translation) gives the
+    reference's coordinates bit for bit (no GPU)."""
+    from conftest import golden
+    from srsoriginal_b200.sr import sr
+    g = golden("points_surface.npz")
+    xyz, nrm = sr._surface_3d(g["points"].tolist(), [2e-5, -3e-5, 0.3], [0.0005, -0.0002, 0.1], False)
+    assert np.array_equal(xyz, g["pd0_coords"])
+    with pytest.raises(ValueError, match="Incorrect format in 'points'"):
+        sr._surface_3d([[[0, 0, 1]]], None, None, False)
+    with pytest.raises(ValueError, match="Point or Normal does not have 3 elements"):
+        sr._surface_3d([[[0, 0], [0, 0, 1]]], None, None, False)
