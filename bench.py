@@ -9,8 +9,9 @@ One step = both flux maps (E1 and E3) in mixed precision from the device-residen
 2 * 20001 * 10201 = 4.08e8 integrand evaluations.  ``value`` is integrand evaluations per second of
 the whole job (all ranks), device-timed with CUDA events per step; the L2 (126 MB) is flushed with a
 256 MiB write before every step, outside the timed events.  ``e2e`` is the same metric through the
-public API (``srsoriginal_b200.sr.sr``: RK4 trajectory on the GPU, host->device copies of the inputs,
-both maps, device->host copy of the results), host wall-clock around synchronous calls.
+public API (``srsoriginal_b200.sr.sr``: RK4 trajectory on the GPU, integrated parallel in time,
+host->device copies of the inputs, both maps, device->host copy of the results), host wall-clock
+around synchronous calls.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -531,7 +532,8 @@ def run_ours(args, world, rank, local):
 
     # e2e through the public API (host buffers, synchronous calls).  One step = what a user does for
     # config 1: the trajectory (RK4 on the GPU, once: the object drops its kept trajectory at the start
-    # of every step) and both maps, with the host<->device copies of each call.
+    # of every step; parallel in time, as the object integrates it for mixed-precision sums) and both
+    # maps, with the host<->device copies of each call.
     o = sr()
     W.setup_beam(o, NT)
     W.setup_undulator(o)
@@ -543,21 +545,30 @@ def run_ours(args, world, rank, local):
             o.flux_arrays(e, [GRID_N, GRID_N], "XY", [WIDTH, WIDTH], translation=[0, 0, W.SCREEN_Z],
                           precision="mixed")
 
-    for _ in range(min(2, args.warmup)):
-        e2e_step()
-    torch.cuda.synchronize()
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    def timed_e2e(steps):
+        for _ in range(min(2, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        return max_over_ranks(time.perf_counter() - t0, world)
+
+    # the same steps with the serial RK4 chain, for comparison (not the reported value)
+    o.set_trajectory_mode("serial")
+    e2e_serial_s = timed_e2e(min(3, e2e_steps))
+    o.set_trajectory_mode("auto")
+    e2e_s = timed_e2e(e2e_steps)
     e2e = {"value": world * EVALS_PER_STEP * e2e_steps / e2e_s, "unit": UNIT,
            # per map: accumulator and compensation arrays in, particle in (RK4 once per step); out: both arrays
            "h2d_bytes_per_step": len(ENERGIES) * 2 * npts * 8 + 56,
            "d2h_bytes_per_step": len(ENERGIES) * 2 * npts * 8,
            "ms_per_step": 1e3 * e2e_s / e2e_steps,
-           "includes": "RK4 trajectory on the GPU (once per step), both maps, host<->device copies of each call"}
+           "includes": "RK4 trajectory on the GPU (once per step, parallel in time), both maps, host<->device "
+                       "copies of each call",
+           "ms_per_step_serial_trajectory": 1e3 * e2e_serial_s / min(3, e2e_steps)}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

@@ -104,6 +104,21 @@ srs_status srs_trajectory(const srs_field *fields, int32_t nfields, const srs_pa
                           int32_t nparticles, double ctstart, double ctstop, double t0, int64_t npoints,
                           double *d_x, double *d_beta, double *d_aoc, void *stream);
 
+/* The trajectory of ONE particle, integrated parallel in time: the serial RK4 chain is cut into
+ * segments of steps_per_segment steps (0 = automatic) whose start states are found by Newton
+ * iterations of multiple shooting, every segment stepping with the same arithmetic as srs_trajectory.
+ * The result equals srs_trajectory's to a few ulps of the positions (~1e-16 m), not bit for bit: it
+ * feeds the mixed-precision sums, while the FP64 drop-in keeps srs_trajectory.  When the iteration
+ * has not converged after max_iterations iterations (0 = 8; at most 32) the serial kernel writes the
+ * trajectory instead (no host synchronisation either way).  d_stats (optional, DEVICE, 4 doubles): converged (1 or 0),
+ * iterations, the last update and the largest mismatch between a segment's end and the next one's
+ * start, both relative to the trajectory's extent (positions) or speed (velocities).
+ * No reference counterpart: the reference integrates serially (OSCARSSR.cc:562-673). */
+srs_status srs_trajectory_shoot(const srs_field *fields, int32_t nfields, const srs_particle *particle,
+                                double ctstart, double ctstop, double t0, int64_t npoints,
+                                int32_t steps_per_segment, int32_t max_iterations, double *d_x,
+                                double *d_beta, double *d_aoc, double *d_stats, void *stream);
+
 /* ------------------------------------------------------------------ radiation sums */
 
 /* Arithmetic of the sums. */
@@ -323,6 +338,13 @@ srs_status srs_sim_clear_bfields(srs_sim *sim);
  * the identical trajectory on every call).  enabled = 0 turns this off; every call drops the kept
  * trajectory.  No counterpart in the reference. */
 srs_status srs_sim_set_trajectory_cache(srs_sim *sim, int32_t enabled);
+/* How the object integrates single-particle trajectories: SRS_TRAJ_AUTO (default) parallel in time
+ * (srs_trajectory_shoot) for the mixed-precision sums and serially (srs_trajectory, the reference's
+ * roundings) for everything else; SRS_TRAJ_SERIAL always serially; SRS_TRAJ_PARALLEL always parallel
+ * in time.  Trajectories shorter than 1024 points and multi-particle batches are always serial.
+ * No counterpart in the reference. */
+enum { SRS_TRAJ_AUTO = 0, SRS_TRAJ_SERIAL = 1, SRS_TRAJ_PARALLEL = 2 };
+srs_status srs_sim_set_trajectory_mode(srs_sim *sim, int32_t mode);
 int32_t srs_sim_get_nfields(srs_sim *sim);
 /* Field at points (evaluated on the device): xyz and out are HOST arrays of 3*np doubles. */
 srs_status srs_sim_get_bfield(srs_sim *sim, const double *xyz, int64_t np, double *out);

@@ -80,6 +80,8 @@ def _load():
                                       C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "srs_trajectory": (S, [C.POINTER(Field), C.c_int32, C.POINTER(Particle), C.c_int32, C.c_double,
                                C.c_double, C.c_double, C.c_int64, P, P, P, P]),
+        "srs_trajectory_shoot": (S, [C.POINTER(Field), C.c_int32, C.POINTER(Particle), C.c_double, C.c_double,
+                                     C.c_double, C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P]),
         "srs_spectrum": (S, [TrajView, BeamConsts, _D, P, C.c_int64, C.c_int32, P, P]),
         "srs_flux": (S, [TrajView, BeamConsts, P, C.c_int64, C.POINTER(Grid2D), C.c_double, C.c_int32,
                          P, P]),
@@ -102,6 +104,7 @@ def _load():
         "srs_sim_add_bfield_grid": (S, [P, _D, _D, C.POINTER(C.c_int64), _D, _D, _D]),
         "srs_sim_clear_bfields": (S, [P]),
         "srs_sim_set_trajectory_cache": (S, [P, C.c_int32]),
+        "srs_sim_set_trajectory_mode": (S, [P, C.c_int32]),
         "srs_sim_get_nfields": (C.c_int32, [P]),
         "srs_sim_get_bfield": (S, [P, _D, C.c_int64, _D]),
         "srs_sim_set_field_grid_data": (S, [P, C.c_int32, P, C.c_int32]),
@@ -152,13 +155,13 @@ def _load():
 
 lib = _load()
 EXPORTED = (
-    "srs_last_error srs_version srs_device_count srs_trajectory_counts srs_trajectory srs_spectrum "
+    "srs_last_error srs_version srs_device_count srs_trajectory_counts srs_trajectory srs_trajectory_shoot srs_spectrum "
     "srs_flux srs_power_density srs_total_power srs_accumulate srs_sim_create srs_sim_destroy "
     "srs_sim_set_ctstartstop srs_sim_set_npoints_trajectory srs_sim_get_ctstartstop "
     "srs_sim_get_npoints_trajectory srs_sim_set_nthreads_global srs_sim_set_gpu_global "
     "srs_sim_add_bfield_undulator srs_sim_add_bfield_gaussian srs_sim_add_bfield_uniform "
     "srs_sim_add_bfield_file srs_sim_add_bfield_grid srs_sim_clear_bfields srs_sim_get_nfields "
-    "srs_sim_set_trajectory_cache "
+    "srs_sim_set_trajectory_cache srs_sim_set_trajectory_mode "
     "srs_sim_get_bfield srs_sim_set_field_grid_data srs_sim_add_particle_beam "
     "srs_sim_clear_particle_beams srs_sim_get_nparticle_beams srs_sim_set_new_particle "
     "srs_sim_get_particle srs_set_seed srs_random_uniform srs_random_normal srs_random_reset "

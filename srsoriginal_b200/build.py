@@ -25,6 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # (source, exact IEEE double: -fmad=false)
 SOURCES = [
     ("rk4.cu", True),
+    ("rk4_shoot.cu", True),
     ("sums_fp64.cu", True),
     ("sums_mixed.cu", False),
     ("queue.cu", False),

@@ -93,6 +93,36 @@ srs_status srs_trajectory(const srs_field *fields, int32_t nfields, const srs_pa
   return SRS_OK;
 }
 
+srs_status srs_trajectory_shoot(const srs_field *fields, int32_t nfields, const srs_particle *particle,
+                                double ctstart, double ctstop, double t0, int64_t npoints,
+                                int32_t steps_per_segment, int32_t max_iterations, double *d_x, double *d_beta,
+                                double *d_aoc, double *d_stats, void *stream) {
+  clear_error();
+  double dt;
+  int64_t nf, nb;
+  srs_status st = srs_trajectory_counts(ctstart, ctstop, t0, npoints, &dt, &nf, &nb);
+  if (st) return st;
+  if (nfields < 0 || (nfields > 0 && !fields)) return fail(SRS_ERR_INVALID, "bad field array");
+  if (!particle) return fail(SRS_ERR_INVALID, "bad particle");
+  if (!d_x || !d_beta || !d_aoc) return fail(SRS_ERR_INVALID, "output pointers are NULL");
+  if (steps_per_segment < 0) return fail(SRS_ERR_INVALID, "steps_per_segment must be >= 0");
+  if (max_iterations < 0 || max_iterations > 32) return fail(SRS_ERR_INVALID, "max_iterations must be in [0, 32]");
+  for (int i = 0; i < nfields; ++i)
+    if (fields[i].kind == SRS_FIELD_GRID && !fields[i].data)
+      return fail(SRS_ERR_INVALID, "grid field without data");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DeviceBuffer df, dp, scratch;
+  SRS_CUDA(df.alloc(sizeof(srs_field) * (nfields > 0 ? nfields : 1), s));
+  SRS_CUDA(dp.alloc(sizeof(srs_particle), s));
+  SRS_CUDA(scratch.alloc(shoot_scratch_bytes(nf, nb, steps_per_segment), s));
+  if (nfields > 0) SRS_CUDA(cudaMemcpyAsync(df.ptr, fields, sizeof(srs_field) * nfields, cudaMemcpyHostToDevice, s));
+  SRS_CUDA(cudaMemcpyAsync(dp.ptr, particle, sizeof(srs_particle), cudaMemcpyHostToDevice, s));
+  SRS_CUDA(launch_rk4_shoot(df.as<srs_field>(), nfields, dp.as<srs_particle>(), *particle, dt, nf, nb, d_x, d_beta,
+                            d_aoc, s, nfields > 0 ? grid_stage_doubles(fields, nfields) : 0, steps_per_segment,
+                            max_iterations, scratch.ptr, d_stats));
+  return SRS_OK;
+}
+
 srs_status srs_spectrum(srs_traj_view traj, srs_beam_consts beam, const double obs[3], const double *d_energies,
                         int64_t ne, int32_t precision, double *d_out, void *stream) {
   clear_error();

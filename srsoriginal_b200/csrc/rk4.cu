@@ -24,135 +24,12 @@
 // first, earliest at index 0), so no reversal pass is needed.
 #include <cuda_runtime.h>
 
-#include "srs_device.cuh"
+#include "rk4_fields.cuh"
 #include "srs_internal.h"
 
 namespace srs {
 
 namespace {
-
-constexpr int kMaxFieldsShared = 16;
-// grid samples staged in shared memory when all grid fields together fit (192 KB)
-constexpr int64_t kGridStageMaxDoubles = 24576;
-
-
-// Field constants the reference derives inside GetF (or in Init) from the descriptor.
-struct Prepared {
-  int kind;
-  double F[3], C[3], u[3];
-  double plen, rplen, ps, taper, b_lo, b_hi, e1_lo, e1_hi, e2_lo, e2_hi;  // undulator
-  double rs[3], rc[3];                                                     // rotation sines / cosines
-  const double *gd;                                                        // grid samples (shared or global)
-  double rstep[3];                                                         // grid: 1 / step per axis
-};
-
-__device__ void prepare(const srs_field &f, Prepared &p) {
-  p.kind = f.kind;
-  p.gd = f.data;
-  for (int c = 0; c < 3; ++c) p.rstep[c] = f.step[c] != 0 ? 1.0 / f.step[c] : 0.0;
-  for (int c = 0; c < 3; ++c) {
-    p.F[c] = f.field[c];
-    p.C[c] = f.center[c];
-    p.rs[c] = sin(f.rotations[c]);
-    p.rc[c] = cos(f.rotations[c]);
-  }
-  if (f.kind == SRS_FIELD_UNDULATOR) {
-    // TField3D_IdealUndulator::Init (:62-80) and the per-call expressions of GetF (:106-139)
-    const V3 per = ld3(f.period);
-    p.plen = mag(per);
-    p.rplen = 1.0 / p.plen;
-    const V3 u = unit(per);
-    p.u[0] = u.x; p.u[1] = u.y; p.u[2] = u.z;
-    const double L = mag(per) * (f.nperiods + 2);
-    p.ps = f.phase * mag(per) / two_pi();
-    p.taper = f.taper;
-    p.b_hi = L / 2. + p.ps;
-    p.b_lo = -L / 2. + p.ps;
-    p.e1_lo = -L / 2. + p.ps + p.plen;
-    p.e1_hi = L / 2. + p.ps - p.plen;
-    p.e2_lo = -L / 2. + p.ps + p.plen / 2.;
-    p.e2_hi = L / 2. + p.ps - p.plen / 2.;
-  }
-}
-
-// RotateSelfXYZ with the angles' sines and cosines precomputed (TVector3D.cc:150-205)
-__device__ inline V3 rotate_pre(V3 v, const Prepared &p) {
-  double t = v.y;
-  v.y = p.rc[0] * t - p.rs[0] * v.z;
-  v.z = p.rs[0] * t + p.rc[0] * v.z;
-  t = v.z;
-  v.z = p.rc[1] * t - p.rs[1] * v.x;
-  v.x = p.rs[1] * t + p.rc[1] * v.x;
-  t = v.x;
-  v.x = p.rc[2] * t - p.rs[2] * v.y;
-  v.y = p.rs[2] * t + p.rc[2] * v.y;
-  return v;
-}
-
-__device__ inline V3 field_one(const Prepared &p, const srs_field &f, V3 X) {
-  switch (p.kind) {
-    case SRS_FIELD_UNDULATOR: {
-      const double D = (X.x - p.C[0]) * p.u[0] + (X.y - p.C[1]) * p.u[1] + (X.z - p.C[2]) * p.u[2];
-      const double taper = 1 + D * p.taper;
-      if (D > p.b_hi || D < p.b_lo) return v3(0, 0, 0);
-      const double s = sin(div_rn(two_pi() * (D - p.ps), p.plen, p.rplen));
-      // ends: 0.25 / 0.75 of the field; the centre multiplies by 1.0, which is exact
-      const double fac = (D < p.e1_lo || D > p.e1_hi) ? ((D < p.e2_lo || D > p.e2_hi) ? 0.25 : 0.75) : 1.0;
-      return v3(p.F[0] * fac * s * taper, p.F[1] * fac * s * taper, p.F[2] * fac * s * taper);
-    }
-    case SRS_FIELD_GAUSSIAN: {
-      const V3 rx = rotate_pre(X, p) - ld3(p.C);
-      double frac = 1;
-      if (f.sigma_or_width[0] > 0) { double t = rx.x / f.sigma_or_width[0]; frac *= exp(-(t * t) / 2.); }
-      if (f.sigma_or_width[1] > 0) { double t = rx.y / f.sigma_or_width[1]; frac *= exp(-(t * t) / 2.); }
-      if (f.sigma_or_width[2] > 0) { double t = rx.z / f.sigma_or_width[2]; frac *= exp(-(t * t) / 2.); }
-      return ld3(p.F) * frac;
-    }
-    case SRS_FIELD_UNIFORM_BOX: {
-      const V3 rx = rotate_pre(X, p) - ld3(p.C);
-      const double *w = f.sigma_or_width;
-      if ((!(w[0] <= 0) && fabs(rx.x) > fabs(w[0] / 2.)) || (!(w[1] <= 0) && fabs(rx.y) > fabs(w[1] / 2.)) ||
-          (!(w[2] <= 0) && fabs(rx.z) > fabs(w[2] / 2.)))
-        return v3(0, 0, 0);
-      return ld3(p.F);
-    }
-    case SRS_FIELD_GRID:  // grid_field with the rotation's sines and cosines precomputed
-      return grid_interp(f, p.gd, rotate_pre(X, p) - ld3(f.translation), p.rstep);
-    default:
-      return v3(0, 0, 0);
-  }
-}
-
-// DerivativesB (OSCARSSR.cc:741-765): the velocity part
-__device__ inline V3 force(double qomg, V3 v, V3 B) {
-  return v3(qomg * (-v.z * B.y + v.y * B.z), qomg * (v.z * B.x - v.x * B.z), qomg * (v.x * B.y - v.y * B.x));
-}
-
-__device__ inline V3 vadd_scaled(V3 a, double h, V3 b) { return v3(a.x + h * b.x, a.y + h * b.y, a.z + h * b.z); }
-
-// Copies every grid field's samples into the block's dynamic shared memory (the launcher sizes it to
-// the total when that fits) and points the prepared fields at the copies: the interpolation then
-// reads shared memory instead of global memory inside the serial RK4 chain.
-extern __shared__ double g_stage[];
-__device__ void stage_grids(const srs_field *sf, Prepared *sp, int nfields) {
-  int64_t off = 0;
-  for (int i = 0; i < nfields; ++i) {
-    if (sf[i].kind != SRS_FIELD_GRID) continue;
-    const int64_t cnt = 3 * sf[i].n[0] * sf[i].n[1] * sf[i].n[2];
-    for (int64_t k = threadIdx.x; k < cnt; k += blockDim.x) g_stage[off + k] = sf[i].data[k];
-    off += cnt;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    off = 0;
-    for (int i = 0; i < nfields; ++i) {
-      if (sf[i].kind != SRS_FIELD_GRID) continue;
-      sp[i].gd = g_stage + off;
-      off += 3 * sf[i].n[0] * sf[i].n[1] * sf[i].n[2];
-    }
-  }
-  __syncthreads();
-}
 
 // ---------------------------------------------------------------- warp-cooperative kernel
 
@@ -169,7 +46,8 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
                                                        double dt_all, int64_t nfwd_all, int64_t nbwd_all,
                                                        double *__restrict__ X, double *__restrict__ Bt,
                                                        double *__restrict__ A, const TrajSpec *__restrict__ specs,
-                                                       int64_t stage_doubles) {
+                                                       int64_t stage_doubles, const int *__restrict__ skip) {
+  if (skip && *skip) return;  // the parallel-in-time integration already wrote this trajectory
   __shared__ srs_field sf[kMaxFieldsShared];
   __shared__ Prepared sp[kMaxFieldsShared];
   __shared__ double sink[128];  // target of the stores a lane does not make (no branch around them)
@@ -405,29 +283,31 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 template <int G>
 static cudaError_t launch_warp_rk4_g(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
                               double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
-                              const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s) {
+                              const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s,
+                              const int *d_skip = nullptr) {
   const size_t smem = sizeof(double) * (size_t)stage_doubles;
   if (cudaError_t e = allow_smem(rk4_warp_kernel<G>, smem)) return e;
   const int warps = 4, per_block = G == 32 ? 1 : warps * (32 / G);
   rk4_warp_kernel<G><<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
-      d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, d_specs, stage_doubles);
+      d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, d_specs, stage_doubles, d_skip);
   return cudaGetLastError();
 }
 
 static cudaError_t launch_warp_rk4(int G, const srs_field *d_fields, int nfields, const srs_particle *d_particles,
                             int nparticles, double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b,
-                            double *d_a, const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s) {
+                            double *d_a, const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s,
+                            const int *d_skip = nullptr) {
   switch (G) {
     case 2: return launch_warp_rk4_g<2>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
-                                        d_specs, stage_doubles, s);
+                                        d_specs, stage_doubles, s, d_skip);
     case 4: return launch_warp_rk4_g<4>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
-                                        d_specs, stage_doubles, s);
+                                        d_specs, stage_doubles, s, d_skip);
     case 8: return launch_warp_rk4_g<8>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
-                                        d_specs, stage_doubles, s);
+                                        d_specs, stage_doubles, s, d_skip);
     case 16: return launch_warp_rk4_g<16>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
-                                          d_specs, stage_doubles, s);
+                                          d_specs, stage_doubles, s, d_skip);
     case 32: return launch_warp_rk4_g<32>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
-                                          d_specs, stage_doubles, s);
+                                          d_specs, stage_doubles, s, d_skip);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -452,6 +332,14 @@ cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particl
         d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, stage_doubles);
   }
   return cudaGetLastError();
+}
+
+cudaError_t launch_rk4_unless(const srs_field *d_fields, int nfields, const srs_particle *d_particles, double dt,
+                              int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a, cudaStream_t s,
+                              int64_t stage_doubles, const int *d_skip) {
+  if (nfields > kMaxFieldsShared) return cudaErrorInvalidValue;
+  return launch_warp_rk4(group_size(1, nfields), d_fields, nfields, d_particles, 1, dt, nfwd, nbwd, d_x, d_b, d_a,
+                         nullptr, stage_doubles, s, d_skip);
 }
 
 cudaError_t launch_rk4_specs(const srs_field *d_fields, int nfields, const srs_particle *d_particles,

@@ -26,6 +26,10 @@
 namespace srs {
 namespace {
 
+// Shortest single-particle trajectory integrated parallel in time (below it the serial chain, at
+// ~0.9 us per step, costs about what the shooting iterations' launches do).
+constexpr int64_t kShootMinPoints = 1024;
+
 // ---------------------------------------------------------------- global random generator
 // TRandomA (src/TRandomA.cc): one process-wide engine seeded from std::random_device; SetSeed
 // replaces the engine but keeps the distributions, so a cached second normal value survives a reseed.
@@ -212,13 +216,14 @@ struct srs_sim {
   // RK4 when the particle, the fields and the trajectory settings are unchanged.
   struct TrajCache {
     bool valid = false;
-    double key[11] = {0};
+    double key[12] = {0};
     uint64_t fields_version = 0;
     double *x = nullptr, *b = nullptr, *a = nullptr;
     int64_t capacity = 0;
     srs_traj_view view{};
   } cache;
   bool cache_enabled = true;
+  int32_t traj_mode = SRS_TRAJ_AUTO;
   std::vector<Beam> beams;
   std::vector<double> weight_sums;
   std::map<std::string, size_t> beam_index;
@@ -317,8 +322,19 @@ struct srs_sim {
     return SRS_OK;
   }
 
+  // Whether the single-particle trajectory of a calculation in this precision is integrated parallel
+  // in time: for the mixed-precision sums in the automatic mode (their error budget, 1e-4, dwarfs the
+  // shooting trajectory's ~1e-16 m), always in the parallel mode, never for the FP64 drop-in path
+  // unless the caller asked for it.
+  bool shoot_for(int32_t precision) const {
+    if (traj_mode == SRS_TRAJ_PARALLEL) return true;
+    return traj_mode == SRS_TRAJ_AUTO && precision == SRS_PRECISION_MIXED;
+  }
+
   // RK4 trajectories of a batch of particles that share t0 into device arrays (layout of srs_trajectory).
-  srs_status integrate(const Particle *ps, int np, double *X, double *B, double *A, srs_traj_view &view) {
+  // shoot: one particle, parallel in time (long trajectories only; short ones are cheaper serially).
+  srs_status integrate(const Particle *ps, int np, double *X, double *B, double *A, srs_traj_view &view,
+                       bool shoot = false) {
     double dt;
     int64_t nf, nb;
     if (srs_status st = srs_trajectory_counts(ctstart, ctstop, ps[0].t0, npoints, &dt, &nf, &nb)) return st;
@@ -334,9 +350,17 @@ struct srs_sim {
     DeviceBuffer dp;
     SRS_CUDA(dp.alloc(sizeof(srs_particle) * np, stream));
     SRS_CUDA(cudaMemcpyAsync(dp.ptr, hp.data(), sizeof(srs_particle) * np, cudaMemcpyHostToDevice, stream));
-    SRS_CUDA(launch_rk4(reinterpret_cast<const srs_field *>(d_fields), (int)fields.size(), dp.as<srs_particle>(), np,
-                        dt, nf, nb, X, B, A, stream,
-                        fields.empty() ? 0 : grid_stage_doubles(fields.data(), (int)fields.size())));
+    const int64_t stage = fields.empty() ? 0 : grid_stage_doubles(fields.data(), (int)fields.size());
+    if (shoot && np == 1 && n >= kShootMinPoints) {
+      DeviceBuffer scratch;
+      SRS_CUDA(scratch.alloc(shoot_scratch_bytes(nf, nb, 0), stream));
+      SRS_CUDA(launch_rk4_shoot(reinterpret_cast<const srs_field *>(d_fields), (int)fields.size(),
+                                dp.as<srs_particle>(), hp[0], dt, nf, nb, X, B, A, stream, stage, 0, 0, scratch.ptr,
+                                nullptr));
+    } else {
+      SRS_CUDA(launch_rk4(reinterpret_cast<const srs_field *>(d_fields), (int)fields.size(), dp.as<srs_particle>(), np,
+                          dt, nf, nb, X, B, A, stream, stage));
+    }
     view.x = X;
     view.beta = B;
     view.aoc = A;
@@ -367,9 +391,9 @@ struct srs_sim {
   }
 
   // The trajectory of one particle, from the cache when nothing it depends on has changed.
-  srs_status single(const Particle &p, srs_traj_view &view) {
-    const double key[11] = {p.x0.x, p.x0.y, p.x0.z, p.b0.x, p.b0.y, p.b0.z, p.qomg, p.t0, ctstart, ctstop,
-                            (double)npoints};
+  srs_status single(const Particle &p, srs_traj_view &view, bool shoot = false) {
+    const double key[12] = {p.x0.x, p.x0.y, p.x0.z, p.b0.x, p.b0.y, p.b0.z, p.qomg, p.t0, ctstart, ctstop,
+                            (double)npoints, shoot ? 1.0 : 0.0};
     if (cache_enabled && cache.valid && cache.fields_version == fields_version && cache.view.n > 0 &&
         std::memcmp(key, cache.key, sizeof key) == 0) {
       int64_t n;
@@ -391,7 +415,7 @@ struct srs_sim {
       for (double **q : {&cache.x, &cache.b, &cache.a}) SRS_CUDA(cudaMalloc(q, sizeof(double) * 3 * (size_t)n));
       cache.capacity = n;
     }
-    if (srs_status st = integrate(&p, 1, cache.x, cache.b, cache.a, cache.view)) return st;
+    if (srs_status st = integrate(&p, 1, cache.x, cache.b, cache.a, cache.view, shoot)) return st;
     std::memcpy(cache.key, key, sizeof key);
     cache.fields_version = fields_version;
     cache.valid = cache_enabled;
@@ -413,7 +437,8 @@ struct srs_sim {
   // The common driver: sample particles, integrate in batches, run `sum` on each batch (writing
   // per-particle values to d_vals), then Kahan-accumulate them in particle order into out/comp.
   template <class SumFn>
-  srs_status run(int32_t nparticles, int64_t nout, double *out, double *comp, bool apply_weight, SumFn sum) {
+  srs_status run(int32_t nparticles, int64_t nout, double *out, double *comp, bool apply_weight, int32_t precision,
+                 SumFn sum) {
     std::vector<Particle> ps;
     double weight;
     if (srs_status st = particles_for(nparticles, ps, weight)) return st;
@@ -434,7 +459,7 @@ struct srs_sim {
       DeviceBuffer X, B, A, vals;
       srs_traj_view view;
       if (nparticles == 0) {
-        if (srs_status st = single(ps[b0], view)) return st;
+        if (srs_status st = single(ps[b0], view, shoot_for(precision))) return st;
       } else if (srs_status st = trajectories(&ps[b0], np, X, B, A, view)) {
         return st;
       }
@@ -595,6 +620,14 @@ srs_status srs_sim_clear_bfields(srs_sim *sim) {
   sim->grid_dev.clear();
   sim->fields_dirty = true;
   ++sim->fields_version;
+  return SRS_OK;
+}
+
+srs_status srs_sim_set_trajectory_mode(srs_sim *sim, int32_t mode) {
+  SIM_GUARD(sim);
+  if (mode != SRS_TRAJ_AUTO && mode != SRS_TRAJ_SERIAL && mode != SRS_TRAJ_PARALLEL)
+    return fail(SRS_ERR_INVALID, "unknown trajectory mode");
+  sim->traj_mode = mode;
   return SRS_OK;
 }
 
@@ -763,7 +796,7 @@ srs_status srs_sim_calculate_trajectory(srs_sim *sim, int64_t *n, double *x, dou
   }
   if (*n != nf + nb) return fail(SRS_ERR_INVALID, "output size does not match the trajectory");
   srs_traj_view v;
-  if (srs_status st = sim->single(sim->particle, v)) return st;
+  if (srs_status st = sim->single(sim->particle, v, sim->shoot_for(SRS_PRECISION_FP64))) return st;
   std::vector<double> hx(3 * v.n), hb(3 * v.n);
   SRS_CUDA(cudaMemcpyAsync(hx.data(), v.x, sizeof(double) * 3 * v.n, cudaMemcpyDeviceToHost, sim->stream));
   SRS_CUDA(cudaMemcpyAsync(hb.data(), v.beta, sizeof(double) * 3 * v.n, cudaMemcpyDeviceToHost, sim->stream));
@@ -786,7 +819,8 @@ srs_status srs_sim_calculate_spectrum(srs_sim *sim, const double obs[3], const d
   SRS_CUDA(cudaMemcpyAsync(de.ptr, energies, sizeof(double) * ne, cudaMemcpyHostToDevice, sim->stream));
   const double *d_e = de.as<double>();
   cudaStream_t s = sim->stream;
-  return sim->run(nparticles, ne, out, comp, true, [&](const srs_traj_view &v, const srs_beam_consts &bc, double *dv) {
+  return sim->run(nparticles, ne, out, comp, true, precision,
+                  [&](const srs_traj_view &v, const srs_beam_consts &bc, double *dv) {
     return srs_spectrum(v, bc, obs, d_e, ne, precision, dv, s);
   });
 }
@@ -804,7 +838,8 @@ srs_status srs_sim_calculate_flux(srs_sim *sim, const double *points, int64_t np
     d_p = dp.as<double>();
   }
   cudaStream_t s = sim->stream;
-  return sim->run(nparticles, np, out, comp, true, [&](const srs_traj_view &v, const srs_beam_consts &bc, double *dv) {
+  return sim->run(nparticles, np, out, comp, true, precision,
+                  [&](const srs_traj_view &v, const srs_beam_consts &bc, double *dv) {
     return srs_flux(v, bc, d_p, np, grid, energy_ev, precision, dv, s);
   });
 }
@@ -826,7 +861,7 @@ srs_status srs_sim_calculate_power_density(srs_sim *sim, const double *points, c
     d_n = d_p + 3 * np;
   }
   cudaStream_t s = sim->stream;
-  return sim->run(nparticles, np, out, comp, weighted != 0,
+  return sim->run(nparticles, np, out, comp, weighted != 0, precision,
                   [&](const srs_traj_view &v, const srs_beam_consts &bc, double *dv) {
                     return srs_power_density(v, bc, d_p, d_n, np, grid, directional, precision, dv, s);
                   });
@@ -837,7 +872,7 @@ srs_status srs_sim_calculate_total_power(srs_sim *sim, double *out) {
   if (!out) return fail(SRS_ERR_INVALID, "NULL output");
   if (srs_status st = sim->ensure_particle()) return st;
   srs_traj_view v;
-  if (srs_status st = sim->single(sim->particle, v)) return st;
+  if (srs_status st = sim->single(sim->particle, v, sim->shoot_for(SRS_PRECISION_FP64))) return st;
   srs_beam_consts bc{sim->particle.q, sim->particle.current};
   return srs_total_power(v, bc, &sim->particle.gamma, out, sim->stream);
 }

@@ -62,6 +62,17 @@ cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particl
                        cudaStream_t s, int64_t stage_doubles);
 cudaError_t launch_rk4_specs(const srs_field *d_fields, int nfields, const srs_particle *d_particles,
                              const TrajSpec *d_specs, int nparticles, cudaStream_t s, int64_t stage_doubles);
+// One particle with the serial warp kernel, which returns at once when *d_skip != 0.
+cudaError_t launch_rk4_unless(const srs_field *d_fields, int nfields, const srs_particle *d_particles, double dt,
+                              int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a, cudaStream_t s,
+                              int64_t stage_doubles, const int *d_skip);
+// One particle parallel in time (rk4_shoot.cu); scratch of shoot_scratch_bytes bytes.
+int shoot_default_steps(int64_t nsteps);
+size_t shoot_scratch_bytes(int64_t nfwd, int64_t nbwd, int steps_per_segment);
+cudaError_t launch_rk4_shoot(const srs_field *d_fields, int nfields, const srs_particle *d_particle,
+                             const srs_particle &host_particle, double dt, int64_t nfwd, int64_t nbwd, double *d_x,
+                             double *d_b, double *d_a, cudaStream_t s, int64_t stage_doubles, int steps_per_segment,
+                             int max_iterations, void *scratch, double *d_stats);
 cudaError_t launch_field_eval(const srs_field *d_fields, int nfields, const double *d_xyz, int64_t np,
                               double *d_out, cudaStream_t s);
 

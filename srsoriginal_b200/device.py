@@ -117,6 +117,22 @@ def trajectory(fields, particles, ctstart, ctstop, t0, npoints, out=None):
     return out
 
 
+def trajectory_shoot(fields, particle, ctstart, ctstop, t0, npoints, steps_per_segment=0, max_iterations=0, out=None,
+                     stats=None):
+    """One particle's trajectory integrated parallel in time (srs_trajectory_shoot).  stats: optional
+    CUDA float64 tensor of 4 (converged, iterations, last update, segment defect)."""
+    import torch
+    dt, nf, nb = counts(ctstart, ctstop, t0, npoints)
+    n = nf + nb
+    if out is None:
+        out = Trajectory(*(torch.empty((1, 3, n), dtype=torch.float64, device="cuda") for _ in range(3)), dt)
+    fa = (_lib.Field * max(1, len(fields)))(*fields)
+    check(lib.srs_trajectory_shoot(fa, len(fields), C.byref(particle), ctstart, ctstop, t0, npoints,
+                                   steps_per_segment, max_iterations, _ptr(out.x), _ptr(out.beta), _ptr(out.aoc),
+                                   _ptr(stats) if stats is not None else None, _stream()))
+    return out
+
+
 def grid2d(grid):
     return grid
 

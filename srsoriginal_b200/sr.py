@@ -199,6 +199,17 @@ class sr:  # noqa: N801  (the reference's type name)
         kept trajectory."""
         check(lib.srs_sim_set_trajectory_cache(self._h, 1 if enabled else 0))
 
+    _TRAJ_MODES = {"auto": 0, "serial": 1, "parallel": 2}
+
+    def set_trajectory_mode(self, mode="auto"):
+        """How single-particle trajectories are integrated: 'auto' (default) parallel in time for the
+        mixed-precision sums and serially, with the reference's roundings, for everything else;
+        'serial' always serially; 'parallel' always parallel in time (multiple shooting: equal to the
+        serial trajectory to ~1e-16 m).  Not in the reference."""
+        if mode not in self._TRAJ_MODES:
+            raise ValueError("'mode' must be one of 'auto', 'serial', 'parallel'")
+        check(lib.srs_sim_set_trajectory_mode(self._h, self._TRAJ_MODES[mode]))
+
     # ------------------------------------------------------------ particle beams
     def add_particle_beam(self, type, name, energy_GeV, d0, x0, sigma_energy_GeV=0.0, t0=0.0, current=0.0,
                           weight=1.0, rotations=None, translation=None, horizontal_direction=None, beta=None,
