@@ -338,6 +338,23 @@ def measure_configs(dev):
     out["cfg0_spectrum"] = {"evals": ev, "fp64_ms": ms, "fp64_evals_per_s": ev / (ms * 1e-3), "mixed_ms": msm,
                             "mixed_evals_per_s": ev / (msm * 1e-3)}
 
+    # the trajectory: serial RK4 chain against the parallel-in-time integration (configs 0/1 and 2)
+    epu = und + [D.undulator([0.6, 0, 0], [0, 0, W.PERIOD], W.NPERIODS, phase=np.pi / 2)]
+    rec = {}
+    for npts, fields in ((NT, und), (40001, epu)):
+        ser = D.trajectory(fields, [part], 0.0, 2.0, 0.0, npts)
+        st = torch.zeros(4, dtype=torch.float64, device=dev)
+        sho = D.trajectory_shoot(fields, part, 0.0, 2.0, 0.0, npts, stats=st)
+        ms_ser = _events_ms(lambda: D.trajectory(fields, [part], 0.0, 2.0, 0.0, npts, out=ser), 3)
+        ms_sho = _events_ms(lambda: D.trajectory_shoot(fields, part, 0.0, 2.0, 0.0, npts, out=sho, stats=st), 5)
+        torch.cuda.synchronize()
+        s = st.cpu().tolist()
+        rec[f"{npts}_points_{len(fields)}_undulators"] = {
+            "serial_ms": ms_ser, "parallel_in_time_ms": ms_sho, "speedup": ms_ser / ms_sho,
+            "newton_iterations": int(s[1]), "converged": bool(s[0]),
+            "max_abs_dx_m": float((sho.x - ser.x).abs().max()), "max_abs_dbeta": float((sho.beta - ser.beta).abs().max())}
+    out["trajectory"] = rec
+
     # config 1's first map as a plain point list (no grid to anchor on): the point-list mixed kernel
     xyz1, _, _, _ = rectangle_points([GRID_N, GRID_N], "XY", [WIDTH, WIDTH], translation=[0, 0, W.SCREEN_Z])
     pts1 = torch.as_tensor(np.ascontiguousarray(xyz1.reshape(-1)), device=dev)

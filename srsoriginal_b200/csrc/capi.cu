@@ -114,7 +114,7 @@ srs_status srs_trajectory_shoot(const srs_field *fields, int32_t nfields, const 
   DeviceBuffer df, dp, scratch;
   SRS_CUDA(df.alloc(sizeof(srs_field) * (nfields > 0 ? nfields : 1), s));
   SRS_CUDA(dp.alloc(sizeof(srs_particle), s));
-  SRS_CUDA(scratch.alloc(shoot_scratch_bytes(nf, nb, steps_per_segment), s));
+  SRS_CUDA(scratch.alloc(shoot_scratch_bytes(nf, nb, steps_per_segment, nfields), s));
   if (nfields > 0) SRS_CUDA(cudaMemcpyAsync(df.ptr, fields, sizeof(srs_field) * nfields, cudaMemcpyHostToDevice, s));
   SRS_CUDA(cudaMemcpyAsync(dp.ptr, particle, sizeof(srs_particle), cudaMemcpyHostToDevice, s));
   SRS_CUDA(launch_rk4_shoot(df.as<srs_field>(), nfields, dp.as<srs_particle>(), *particle, dt, nf, nb, d_x, d_beta,

@@ -353,7 +353,7 @@ struct srs_sim {
     const int64_t stage = fields.empty() ? 0 : grid_stage_doubles(fields.data(), (int)fields.size());
     if (shoot && np == 1 && n >= kShootMinPoints) {
       DeviceBuffer scratch;
-      SRS_CUDA(scratch.alloc(shoot_scratch_bytes(nf, nb, 0), stream));
+      SRS_CUDA(scratch.alloc(shoot_scratch_bytes(nf, nb, 0, (int)fields.size()), stream));
       SRS_CUDA(launch_rk4_shoot(reinterpret_cast<const srs_field *>(d_fields), (int)fields.size(),
                                 dp.as<srs_particle>(), hp[0], dt, nf, nb, X, B, A, stream, stage, 0, 0, scratch.ptr,
                                 nullptr));

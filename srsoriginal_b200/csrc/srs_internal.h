@@ -68,7 +68,7 @@ cudaError_t launch_rk4_unless(const srs_field *d_fields, int nfields, const srs_
                               int64_t stage_doubles, const int *d_skip);
 // One particle parallel in time (rk4_shoot.cu); scratch of shoot_scratch_bytes bytes.
 int shoot_default_steps(int64_t nsteps);
-size_t shoot_scratch_bytes(int64_t nfwd, int64_t nbwd, int steps_per_segment);
+size_t shoot_scratch_bytes(int64_t nfwd, int64_t nbwd, int steps_per_segment, int nfields);
 cudaError_t launch_rk4_shoot(const srs_field *d_fields, int nfields, const srs_particle *d_particle,
                              const srs_particle &host_particle, double dt, int64_t nfwd, int64_t nbwd, double *d_x,
                              double *d_b, double *d_a, cudaStream_t s, int64_t stage_doubles, int steps_per_segment,
