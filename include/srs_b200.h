@@ -111,8 +111,9 @@ srs_status srs_trajectory(const srs_field *fields, int32_t nfields, const srs_pa
  * feeds the mixed-precision sums, while the FP64 drop-in keeps srs_trajectory.  When the iteration
  * has not converged after max_iterations iterations (0 = 8; at most 32) the serial kernel writes the
  * trajectory instead (no host synchronisation either way).  d_stats (optional, DEVICE, 4 doubles): converged (1 or 0),
- * iterations, the last update and the largest mismatch between a segment's end and the next one's
- * start, both relative to the trajectory's extent (positions) or speed (velocities).
+ * iterations, and the largest mismatch between a segment's end and the next one's start in the last
+ * and in the previous iteration, relative to the trajectory's extent (positions) or speed (velocities);
+ * the stored trajectory's is the last one's (below 2^-51 when converged).
  * No reference counterpart: the reference integrates serially (OSCARSSR.cc:562-673). */
 srs_status srs_trajectory_shoot(const srs_field *fields, int32_t nfields, const srs_particle *particle,
                                 double ctstart, double ctstop, double t0, int64_t npoints,

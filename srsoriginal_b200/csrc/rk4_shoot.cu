@@ -5,26 +5,31 @@
 // width.  Here each of the reference's two chains (forward from t0 with +dt, backward with -dt;
 // OSCARSSR.cc:562-673) is cut into segments of L steps, and the start state U_n of every segment
 // (U_0 = the initial state, fixed) is found by Newton's method on the matching conditions
-// U_{n+1} = F_n(U_n), F_n = L serial steps.  One iteration is
-//   (1) shoot_fine_kernel: all segments run their L steps from U_n at once, G lanes per segment as in
-//       the serial warp kernel (two rounds of two field evaluations per step, shuffles to combine),
-//       giving F_n(U_n).  While the updates are large, lanes 0..5 also carry the six unit tangents of
-//       the start state (single precision, with the field's Jacobian shuffled from the lanes that
-//       evaluate it), giving the segment's 6 x 6 Jacobian Phi_n.  Each block is a chunk of
-//       consecutive segments and composes their affine maps delta_n -> delta_{n+1} =
-//       (F_n - U_{n+1}) + Phi_n delta_n into one chunk map (M_c, b_c).
-//   (2) shoot_update_kernel: one warp per chain carries delta across the chunk maps (delta = 0 at the
-//       chain's start), then every chunk expands its segments: U'_{n+1} = F_n + Phi_n delta_n, exactly
-//       F_n when delta_n = 0, so segments whose start is already exact stay exact.
-// Once the largest update is small (2^-20 of the trajectory's scale) the Jacobians are kept (a chord
-// step) and the fine kernel, without tangents, also stores the points of the trajectory it integrates;
-// the iteration has converged when the largest update falls below 2^-48 of the scale, and the points
-// stored in that iteration are the trajectory.  If it has not converged after the iteration limit the
-// serial kernel writes the trajectory instead (it exits at once otherwise): no host synchronisation.
+// U_{n+1} = F_n(U_n), F_n = L serial steps.  One Newton iteration is one launch of shoot_pass_kernel,
+// whose blocks are chunks of consecutive segments:
+//   (1) each block first applies the previous iteration's update to its chunk: from the update
+//       delta at the chunk's start (carried by the sweep, below), U'_{n+1} = F_n + Phi_n delta_n for
+//       the chunk's segments in order (exactly F_n when delta_n = 0, so exact starts stay exact);
+//   (2) all segments run their L steps from U_n at once, G lanes per segment as in the serial warp
+//       kernel (two rounds of two field evaluations per step, shuffles to combine), giving F_n(U_n)
+//       and the mismatch r_n = F_n(U_n) - U_{n+1}.  While the mismatches are large, lanes 0..5 also
+//       carry the six unit tangents of the start state (single precision, with the field's Jacobian
+//       shuffled from the lanes that evaluate it), giving the segment's 6 x 6 Jacobian Phi_n; then the
+//       block composes its segments' affine maps delta_n -> delta_{n+1} = r_n + Phi_n delta_n into one
+//       chunk map (M_c, b_c);
+//   (3) the last block to finish (an atomic ticket; nothing waits) adds the mismatches at the chunk
+//       boundaries, decides, and carries delta across the chunk maps (one warp per chain, delta = 0 at
+//       the chain's start) for the next launch.
+// Once the largest mismatch is small (2^-20 of the trajectory's scale) the Jacobians are kept (chord
+// steps) and the passes, without tangents, store the points of the trajectory they integrate; the
+// iteration has converged when a storing pass's largest mismatch is below 2^-51 of the scale (a
+// velocity mismatch of a few ulps, left at every segment boundary, would drift the positions by
+// ~1e-14 m): its stored points are the trajectory.  If it has not converged after the iteration limit the serial
+// kernel writes the trajectory instead (it exits at once otherwise): no host synchronisation.
 // Initial guess: straight flight from the initial state.
 //
 // The stored trajectory equals the serial one up to the ulps by which a start state a few ulps away
-// rounds differently (~1e-16 m), not bit for bit; the FP64 drop-in path keeps the serial kernel.
+// rounds differently (~1e-15 m), not bit for bit; the FP64 drop-in path keeps the serial kernel.
 #include <cuda_runtime.h>
 
 #include "rk4_fields.cuh"
@@ -33,12 +38,11 @@
 namespace srs {
 namespace {
 
-constexpr int kShootThreads = 128;  // threads per fine block: 128 / G segments form one chunk
+constexpr int kShootThreads = 128;  // threads per block: 128 / G segments form one chunk
 constexpr int kMaxIters = 32;       // capacity of the per-iteration record
 constexpr int kDefaultIters = 8;
-constexpr double kTol = 3.552713678800501e-15;  // 2^-48: converged
+constexpr double kTol = 4.440892098500626e-16;  // 2^-51 (~2 ulps of the speed): converged
 constexpr double kNear = 9.5367431640625e-07;   // 2^-20: keep the Jacobians, store the points
-constexpr int kTile = 32;                        // chunk maps staged per chain in the update kernel
 
 struct Plan {
   int64_t mf, mb;         // steps of each chain
@@ -71,24 +75,41 @@ __device__ inline Seg seg_of(const Plan &P, int g) {
   return s;
 }
 
-// flags: [0] converged, [1] iterations run, [2] near (Jacobians kept, points stored), [3] the last fine
-// run stored the points.  diag: [it] largest update of iteration it; [kMaxIters] largest mismatch
-// |F_n(U_n) - U_{n+1}| of the last pass that stored points (both relative to the scales).
-__global__ void shoot_init_kernel(Plan P, const srs_particle *__restrict__ part, double *__restrict__ U,
-                                  int *__restrict__ flags, double *__restrict__ diag) {
+// Device scratch of one integration.
+struct Scratch {
+  double *U, *F, *Phi;     // per segment: start state, end state, Jacobian (row-major 6 x 6)
+  double *Mc, *bc, *dstart;  // per chunk: map (b without the boundary mismatch until the sweep), delta at its start
+  double *Mp, *bp;         // per chunk: the map up to its last segment's start
+  double *diag;            // [it]: largest mismatch of iteration it (relative to the scales)
+  double *rmax;            // this launch's largest interior mismatch (reset by the last block)
+  int *flags;              // [0] converged, [1] iterations, [2] near, [3] the last pass stored, [4] ticket
+  double scale_pos, scale_vel;
+};
+
+__global__ void shoot_init_kernel(Plan P, const srs_particle *__restrict__ part, Scratch W) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g == 0) {
-    for (int k = 0; k < 4; ++k) flags[k] = 0;
-    for (int k = 0; k < kMaxIters + 1; ++k) diag[k] = 0.0;
+    for (int k = 0; k < 5; ++k) W.flags[k] = 0;
+    for (int k = 0; k < kMaxIters; ++k) W.diag[k] = 0.0;
+    *W.rmax = 0.0;
   }
   if (g >= P.sfp + P.sbp) return;
   const Seg s = seg_of(P, g);
   const double C = kC, t = (double)s.j0 * s.h;
   for (int c = 0; c < 3; ++c) {
     const double v = part->beta0[c] * C;
-    U[6 * g + c] = !s.active ? 0.0 : s.j0 == 0 ? part->x0[c] : part->x0[c] + v * t;
-    U[6 * g + 3 + c] = s.active ? v : 0.0;
+    W.U[6 * g + c] = !s.active ? 0.0 : s.j0 == 0 ? part->x0[c] : part->x0[c] + v * t;
+    W.U[6 * g + 3 + c] = s.active ? v : 0.0;
   }
+}
+
+// sum_k a[k * stride] b[k * bstride] over 6 terms as a tree (depth 4 instead of 6: the sweeps are
+// chains of these, and a dependent FP64 operation costs tens of cycles)
+__device__ __forceinline__ double dot6(const double *a, int stride, const double *b, int bstride) {
+  const double p0 = a[0] * b[0], p1 = a[stride] * b[bstride], p2 = a[2 * stride] * b[2 * bstride];
+  const double p3 = a[3 * stride] * b[3 * bstride], p4 = a[4 * stride] * b[4 * bstride];
+  const double p5 = a[5 * stride] * b[5 * bstride];
+  return ((p0 + p1) + (p2 + p3)) + (p4 + p5);
 }
 
 struct F3 {
@@ -104,39 +125,80 @@ __device__ inline F3 fmatvec(const float J[9], F3 d) {
             J[6] * d.x + J[7] * d.y + J[8] * d.z);
 }
 
-// One fine pass.  kTan: tangents and Jacobians (iterations far from convergence); otherwise the
-// points are stored.  final_pass: the store pass after an iteration that converged without storing.
+// One pass over all segments (see the file comment).  kTan: tangents and Jacobians (far from
+// convergence), otherwise the points are stored.  final_pass: the store pass after an iteration that
+// converged without storing (no update, no decision).
+template <int M>
+struct PassShared {
+  srs_field sf[kMaxFieldsShared];
+  Prepared sp[kMaxFieldsShared];
+  double sPhi[M][36], sR[M][6], sU[M + 1][6], sF[M][6], sM[2][36], sB[2][6];
+  double wred[kShootThreads / 32];
+  int am_last, done;
+};
+
 template <int G, bool kTan>
-__global__ void __launch_bounds__(kShootThreads) shoot_fine_kernel(
-    const srs_field *__restrict__ gfields, int nfields, const srs_particle *__restrict__ part, Plan P,
-    const double *__restrict__ U, double *__restrict__ F, double *__restrict__ Phi, double *__restrict__ Mc,
-    double *__restrict__ bc, int *__restrict__ flags, double *__restrict__ defect, double scale_pos, double scale_vel,
-    double *__restrict__ X, double *__restrict__ Bt, double *__restrict__ A, int64_t stage_doubles, int final_pass) {
-  if (final_pass) {
-    if (!flags[0] || flags[3]) return;
-  } else if (flags[0] || (flags[2] != 0) == kTan) {
-    return;  // converged, or the other kind of pass is due (uniform over the grid)
-  }
+__device__ __forceinline__ void shoot_pass(PassShared<kShootThreads / G> &sh, const srs_field *__restrict__ gfields,
+                                           int nfields, const srs_particle *__restrict__ part, const Plan &P,
+                                           const Scratch &W, double *__restrict__ X, double *__restrict__ Bt,
+                                           double *__restrict__ A, int64_t stage_doubles, bool final_pass) {
   constexpr int M = kShootThreads / G;  // segments per block (one chunk)
-  __shared__ srs_field sf[kMaxFieldsShared];
-  __shared__ Prepared sp[kMaxFieldsShared];
-  __shared__ double sPhi[M][36], sR[M][6], sM[2][36], sB[2][6];
-  for (int i = threadIdx.x; i < nfields; i += blockDim.x) {
+  srs_field *const sf = sh.sf;
+  Prepared *const sp = sh.sp;
+  auto &sPhi = sh.sPhi;
+  auto &sR = sh.sR;
+  auto &sU = sh.sU;
+  auto &sF = sh.sF;
+  auto &sM = sh.sM;
+  auto &sB = sh.sB;
+  auto &wred = sh.wred;
+  int &am_last = sh.am_last;
+  int &done = sh.done;
+  const int t = threadIdx.x, lane = t & 31, gl = lane & (G - 1), gbase = lane - gl, grp = t / G;
+  const int c = blockIdx.x, g0 = c * M, g = g0 + grp;
+  const int iter = W.flags[1];
+  const unsigned full = 0xffffffffu;
+  for (int i = t; i < nfields; i += blockDim.x) {
     sf[i] = gfields[i];
     prepare(sf[i], sp[i]);
   }
+  // (1) this chunk's start states: the previous iteration's update, segment after segment (the first
+  // segment's was set by the last block's sweep)
+  for (int k = t; k < M * 6; k += blockDim.x) sU[k / 6][k % 6] = W.U[6 * g0 + k];
+  if (iter > 0 && !final_pass) {
+    for (int k = t; k < M * 36; k += blockDim.x) sPhi[k / 36][k % 36] = W.Phi[36 * g0 + k];
+    for (int k = t; k < M * 6; k += blockDim.x) sF[k / 6][k % 6] = W.F[6 * g0 + k];
+  }
   __syncthreads();
-  if (stage_doubles > 0) stage_grids(sf, sp, nfields);
-  const int lane = threadIdx.x & 31, gl = lane & (G - 1), gbase = lane - gl, grp = threadIdx.x / G;
-  const int g = blockIdx.x * M + grp;
+  if (iter > 0 && !final_pass && t < 32) {  // one warp; lane i < 6 owns component i of delta
+    const int i = lane < 6 ? lane : 0;
+    double d = W.dstart[6 * c + i];
+    for (int n = 0; n + 1 < M; ++n) {
+      const Seg S = seg_of(P, g0 + n);
+      double dl[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) dl[k] = __shfl_sync(full, d, k);
+      if (S.active && !S.last) {
+        const double unew = sF[n][i] + dot6(&sPhi[n][6 * i], 1, dl, 1);  // = F_n exactly when delta_n = 0
+        d = unew - sU[n + 1][i];
+        __syncwarp();
+        if (lane < 6) sU[n + 1][i] = unew;
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  if (!final_pass)
+    for (int k = t; k < M * 6; k += blockDim.x) W.U[6 * g0 + k] = sU[k / 6][k % 6];
+  if (stage_doubles > 0) stage_grids(sf, sp, nfields);  // (ends with a barrier)
+
+  // (2) integrate
   const Seg S = seg_of(P, g);
   const int slot = nfields > 0 ? (gl / nfields) & 1 : 0, fidx = nfields > 0 ? gl % nfields : 0;
   const Prepared myp = sp[fidx];  // this lane's field constants, in registers for the serial chain
   const srs_field &ff = sf[fidx];
   const double C = kC, rC = 1.0 / C, qomg = part->qomg;
   const float qf = (float)qomg;
-  const unsigned full = 0xffffffffu;
-
   // B (exact, summed in field order as the serial kernels do) and, with tangents, the FP32 Jacobian
   // at the two positions of a round
   auto fields2 = [&](V3 pa, V3 pb, V3 &Ba, V3 &Bb, float *Ja, float *Jb) {
@@ -166,17 +228,16 @@ __global__ void __launch_bounds__(kShootThreads) shoot_fine_kernel(
   auto store = [&](int64_t k, V3 pos, V3 vel, V3 acc) {
 #pragma unroll
     for (int r = 0; r < (9 + G - 1) / G; ++r) {
-      const int c = gl + r * G;
-      if (c >= 9) break;
-      const int l3 = c % 3;
-      const V3 src = c < 3 ? pos : c < 6 ? vel : acc;
+      const int cc = gl + r * G;
+      if (cc >= 9) break;
+      const int l3 = cc % 3;
+      const V3 src = cc < 3 ? pos : cc < 6 ? vel : acc;
       const double v = l3 == 0 ? src.x : l3 == 1 ? src.y : src.z;
-      double *const o = (c < 3 ? X : c < 6 ? Bt : A) + (int64_t)l3 * P.n + k;
-      *o = c < 3 ? v : div_rn(v, C, rC);
+      double *const o = (cc < 3 ? X : cc < 6 ? Bt : A) + (int64_t)l3 * P.n + k;
+      *o = cc < 3 ? v : div_rn(v, C, rC);
     }
   };
-
-  V3 pos = ld3(U + 6 * g), vel = ld3(U + 6 * g + 3);
+  V3 pos = ld3(&sU[grp][0]), vel = ld3(&sU[grp][3]);
   F3 dp = f3(gl == 0, gl == 1, gl == 2), dv = f3(gl == 3, gl == 4, gl == 5);
   V3 opos = pos, ovel = vel;
   F3 odp = dp, odv = dv;
@@ -233,36 +294,34 @@ __global__ void __launch_bounds__(kShootThreads) shoot_fine_kernel(
     }
   }
   if (final_pass) return;
-  if (threadIdx.x == 0 && blockIdx.x == 0) flags[3] = kTan ? 0 : 1;
 
-  // F_n; Phi_n (column gl from tangent lane gl); the chunk's map from them and r_n = F_n - U_{n+1}
+  // (3) F_n, the interior mismatches r_n = F_n - U_{n+1} (the chunk's last segment's successor belongs
+  // to the next chunk: the last block adds that one), Phi_n (column gl from tangent lane gl)
   const bool link = S.active && !S.last;  // segment n has a successor to match
   double mis = 0.0;
   if (gl < 6) {
     const double fo[6] = {opos.x, opos.y, opos.z, ovel.x, ovel.y, ovel.z};
-    F[6 * g + gl] = fo[gl];
-    const double r = link ? fo[gl] - U[6 * (g + 1) + gl] : 0.0;
+    W.F[6 * g + gl] = fo[gl];
+    const double r = link && grp + 1 < M ? fo[gl] - sU[grp + 1][gl] : 0.0;
     sR[grp][gl] = r;
-    mis = fabs(r) / (gl < 3 ? scale_pos : scale_vel);
+    mis = fabs(r) / (gl < 3 ? W.scale_pos : W.scale_vel);
     if (kTan) {
       const double col[6] = {odp.x, odp.y, odp.z, odv.x, odv.y, odv.z};
       for (int i = 0; i < 6; ++i) {
         const double v = link ? col[i] : (i == gl ? 1.0 : 0.0);
-        Phi[36 * g + 6 * i + gl] = v;
+        W.Phi[36 * g + 6 * i + gl] = v;
         sPhi[grp][6 * i + gl] = v;
       }
     }
   }
-  if (!kTan) {  // the mismatch of the stored trajectory's segments; the Jacobians of the last tangent pass
-    for (int o = 16; o > 0; o >>= 1) mis = fmax(mis, __shfl_xor_sync(full, mis, o));
-    if (lane == 0 && mis > 0.0)
-      atomicMax(reinterpret_cast<unsigned long long *>(defect), (unsigned long long)__double_as_longlong(mis));
-    for (int k = threadIdx.x; k < M * 36; k += blockDim.x) sPhi[k / 36][k % 36] = Phi[36 * (blockIdx.x * M) + k];
-  }
+  for (int o = 16; o > 0; o >>= 1) mis = fmax(mis, __shfl_xor_sync(full, mis, o));
+  if (lane == 0 && mis > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long *>(W.rmax), (unsigned long long)__double_as_longlong(mis));
+  if (!kTan)  // the Jacobians of the last pass with tangents
+    for (int k = t; k < M * 36; k += blockDim.x) sPhi[k / 36][k % 36] = W.Phi[36 * g0 + k];
   __syncthreads();
   // compose M <- Phi_n M, b <- r_n + Phi_n b over the chunk's segments in order (threads 0..35 own an
   // entry of M, threads 36..41 an entry of b; M is unchanged without new Jacobians)
-  const int t = threadIdx.x;
   const int ti = t < 36 ? t / 6 : t - 36, tj = t % 6;
   if (t < 36) sM[0][t] = ti == tj ? 1.0 : 0.0;
   if (t >= 36 && t < 42) sB[0][ti] = 0.0;
@@ -270,108 +329,140 @@ __global__ void __launch_bounds__(kShootThreads) shoot_fine_kernel(
   int cur = 0;
   for (int n = 0; n < M; ++n) {
     if (kTan && t < 36) {
-      double acc = sPhi[n][6 * ti] * sM[cur][tj];
-      for (int k = 1; k < 6; ++k) acc = acc + sPhi[n][6 * ti + k] * sM[cur][6 * k + tj];
-      sM[cur ^ 1][t] = acc;
+      sM[cur ^ 1][t] = dot6(&sPhi[n][6 * ti], 1, &sM[cur][tj], 6);
     }
     if (t >= 36 && t < 42) {
-      double acc = sPhi[n][6 * ti] * sB[cur][0];
-      for (int k = 1; k < 6; ++k) acc = acc + sPhi[n][6 * ti + k] * sB[cur][k];
-      sB[cur ^ 1][ti] = sR[n][ti] + acc;
+      sB[cur ^ 1][ti] = sR[n][ti] + dot6(&sPhi[n][6 * ti], 1, sB[cur], 1);
     }
     __syncthreads();
     cur ^= 1;
+    if (n == M - 2) {  // the map up to the last segment's start
+      if (kTan && t < 36) W.Mp[36 * c + t] = sM[cur][t];
+      if (t >= 36 && t < 42) W.bp[6 * c + ti] = sB[cur][ti];
+    }
   }
-  if (kTan && t < 36) Mc[36 * blockIdx.x + t] = sM[cur][t];
-  if (t >= 36 && t < 42) bc[6 * blockIdx.x + ti] = sB[cur][ti];
-}
+  if (kTan && t < 36) W.Mc[36 * c + t] = sM[cur][t];
+  if (t >= 36 && t < 42) W.bc[6 * c + ti] = sB[cur][ti];
 
-// Carries delta across the chunk maps (one warp per chain; delta = 0 at the start of a chain), then
-// expands every chunk: U'_{n+1} = F_n + Phi_n delta_n, delta_{n+1} = U'_{n+1} - U_{n+1}.  The largest
-// |delta| relative to the scales decides: converged (kTol), near (kNear).
-__global__ void __launch_bounds__(1024) shoot_update_kernel(Plan P, double *__restrict__ U,
-                                                            const double *__restrict__ F,
-                                                            const double *__restrict__ Phi,
-                                                            const double *__restrict__ Mc,
-                                                            const double *__restrict__ bc, double *__restrict__ dstart,
-                                                            int *__restrict__ flags, double *__restrict__ diag,
-                                                            double scale_pos, double scale_vel) {
-  if (flags[0]) return;
-  __shared__ double tM[2][kTile][36], tb[2][kTile][6];
-  __shared__ double wmax[32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const unsigned full = 0xffffffffu;
-  const int c0 = P.sfp / P.m, c1 = P.sbp / P.m;  // chunks of each chain
-  const int ntile = ((c0 > c1 ? c0 : c1) + kTile - 1) / kTile;
-  double d = 0.0;  // warp w < 2: component `lane` (< 6) of delta at the current chunk start of chain w
-  for (int tt = 0; tt < ntile; ++tt) {
-    for (int k = threadIdx.x; k < 2 * kTile * 42; k += blockDim.x) {
-      const int ch = k / (kTile * 42), r = k % (kTile * 42), q = r / 42, e = r % 42;
-      const int cl = tt * kTile + q, cn = ch == 0 ? c0 : c1, cg = (ch == 0 ? 0 : c0) + cl;
-      if (cl < cn) {
-        if (e < 36) tM[ch][q][e] = Mc[36 * cg + e];
-        else tb[ch][q][e - 36] = bc[6 * cg + e - 36];
-      }
+  // the last block to finish decides and sweeps (the others' writes are fenced before their ticket)
+  __threadfence();
+  __syncthreads();
+  if (t == 0) am_last = atomicAdd(&W.flags[4], 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  const int c0 = P.sfp / P.m, c1 = P.sbp / P.m, nch = c0 + c1;  // chunks of each chain
+  // the boundary mismatches: chunk c's last segment against chunk c + 1's first start state
+  double bm = 0.0;
+  for (int k = t; k < nch * 6; k += blockDim.x) {
+    const int cc = k / 6, i = k % 6, gl_ = cc * M + M - 1;
+    const Seg SL = seg_of(P, gl_);
+    if (SL.active && !SL.last) {
+      const double r = __ldcg(W.F + 6 * gl_ + i) - __ldcg(W.U + 6 * (gl_ + 1) + i);
+      W.bc[6 * cc + i] = __ldcg(W.bc + 6 * cc + i) + r;
+      bm = fmax(bm, fabs(r) / (i < 3 ? W.scale_pos : W.scale_vel));
     }
-    __syncthreads();
-    if (w < 2) {
-      const int cn = w == 0 ? c0 : c1, first = w == 0 ? 0 : c0;
-      const int i = lane < 6 ? lane : 0;
-      for (int q = 0; q < kTile && tt * kTile + q < cn; ++q) {
-        const int cl = tt * kTile + q;
-        if (lane < 6) dstart[6 * (first + cl) + lane] = d;
-        double dl[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) dl[k] = __shfl_sync(full, d, k);
-        double acc = tM[w][q][6 * i] * dl[0];
-#pragma unroll
-        for (int k = 1; k < 6; ++k) acc = acc + tM[w][q][6 * i + k] * dl[k];
-        d = tb[w][q][i] + acc;
-      }
-    }
-    __syncthreads();
   }
-  // expansion: a group of 8 threads per chunk, lane i < 6 owns component i
-  const int gi = threadIdx.x & 7, gb = lane & ~7, i = gi < 6 ? gi : 0;
-  const double rscale = 1.0 / (i < 3 ? scale_pos : scale_vel);
-  double mx = 0.0;
-  const int nchunks = c0 + c1, groups = blockDim.x / 8;
-  for (int cb = 0; cb < nchunks; cb += groups) {  // warp-uniform trip count
-    const int c = cb + (int)(threadIdx.x >> 3);
-    const bool ok = c < nchunks;
-    double dd = ok ? dstart[6 * c + i] : 0.0;
-    for (int n = 0; n < P.m; ++n) {
-      const int g = c * P.m + n;
-      const Seg S = seg_of(P, ok ? g : 0);
-      const bool link = ok && S.active && !S.last;
+  for (int o = 16; o > 0; o >>= 1) bm = fmax(bm, __shfl_xor_sync(full, bm, o));
+  if (lane == 0) wred[t >> 5] = bm;
+  __threadfence();  // the chunk maps' boundary terms, read back through L2 by the sweep
+  __syncthreads();
+  if (t == 0) {
+    double m = __longlong_as_double((long long)atomicAdd(reinterpret_cast<unsigned long long *>(W.rmax), 0ull));
+    for (int k = 0; k < kShootThreads / 32; ++k) m = fmax(m, wred[k]);
+    W.diag[iter < kMaxIters ? iter : kMaxIters - 1] = m;
+    W.flags[1] = iter + 1;
+    W.flags[3] = kTan ? 0 : 1;
+    if (m <= kNear) W.flags[2] = 1;
+    done = m <= kTol;
+    if (done) W.flags[0] = 1;
+    *W.rmax = 0.0;
+    W.flags[4] = 0;
+  }
+  __syncthreads();
+  if (done) return;
+  // carry delta across the chunk maps: warp w < 2 sweeps chain w, lane i < 6 owns component i; the
+  // maps are read three chunks ahead into registers (each of three buffers keeps its role, so a
+  // buffer's loads are consumed three chunks after they are issued)
+  const int w = t >> 5;
+  if (w < 2) {
+    const int cn = w == 0 ? c0 : c1, first = w == 0 ? 0 : c0;
+    const int i = lane < 6 ? lane : 0;
+    auto fetch = [&](int q, double *v) {
+      const int cg = first + q;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) v[k] = __ldcg(W.Mc + 36 * cg + 6 * i + k);
+      v[6] = __ldcg(W.bc + 6 * cg + i);
+    };
+    double d = 0.0;
+    auto step = [&](int q, const double *v) {
+      if (lane < 6) W.dstart[6 * (first + q) + lane] = d;
       double dl[6];
 #pragma unroll
-      for (int k = 0; k < 6; ++k) dl[k] = __shfl_sync(full, dd, gb + k);
-      if (link) {
-        double acc = Phi[36 * g + 6 * i] * dl[0];
+      for (int k = 0; k < 6; ++k) dl[k] = __shfl_sync(full, d, k);
+      d = v[6] + dot6(v, 1, dl, 1);
+    };
+    double b0[7], b1[7], b2[7];
+    if (cn > 0) fetch(0, b0);
+    if (cn > 1) fetch(1, b1);
+    if (cn > 2) fetch(2, b2);
+    for (int q = 0; q < cn; q += 3) {
+      step(q, b0);
+      if (q + 3 < cn) fetch(q + 3, b0);
+      if (q + 1 < cn) step(q + 1, b1);
+      if (q + 4 < cn) fetch(q + 4, b1);
+      if (q + 2 < cn) step(q + 2, b2);
+      if (q + 5 < cn) fetch(q + 5, b2);
+    }
+  }
+  __threadfence_block();
+  __syncthreads();
+  // every chunk, in parallel: delta at its last segment's start (the map up to there) and the next
+  // chunk's first start state U' = F_last + Phi_last delta_last (exactly F_last when delta_last = 0)
+  {
+    const int gi = t & 7, gb = lane & ~7, i = gi < 6 ? gi : 0;
+    for (int cb = 0; cb < nch; cb += kShootThreads / 8) {  // warp-uniform trip count
+      const int cg = cb + (t >> 3), gl_ = cg * M + M - 1;
+      const bool ok = cg < nch;
+      double dl[6], e[6], v[6];
+      double d0 = 0.0, dlast = 0.0;
+      if (ok) {
+        d0 = W.dstart[6 * cg + i];
 #pragma unroll
-        for (int k = 1; k < 6; ++k) acc = acc + Phi[36 * g + 6 * i + k] * dl[k];
-        const double unew = F[6 * g + i] + acc;  // = F_n exactly when delta_n = 0
-        dd = unew - U[6 * (g + 1) + i];
-        if (gi < 6) {
-          U[6 * (g + 1) + i] = unew;
-          mx = fmax(mx, fabs(dd) * rscale);
+        for (int k = 0; k < 6; ++k) e[k] = __ldcg(W.Mp + 36 * cg + 6 * i + k);
+      }
+#pragma unroll
+      for (int k = 0; k < 6; ++k) dl[k] = __shfl_sync(full, d0, gb + k);
+      if (ok) dlast = __ldcg(W.bp + 6 * cg + i) + dot6(e, 1, dl, 1);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) dl[k] = __shfl_sync(full, dlast, gb + k);
+      if (ok) {
+        const Seg SL = seg_of(P, gl_);
+        if (gi < 6 && SL.active && !SL.last) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) v[k] = __ldcg(W.Phi + 36 * gl_ + 6 * i + k);
+          W.U[6 * (gl_ + 1) + i] = __ldcg(W.F + 6 * gl_ + i) + dot6(v, 1, dl, 1);
         }
       }
     }
   }
-  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(full, mx, o));
-  if (lane == 0) wmax[w] = mx;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double m = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = fmax(m, wmax[k]);
-    const int it = flags[1];
-    diag[it < kMaxIters ? it : kMaxIters - 1] = m;
-    flags[1] = it + 1;
-    if (m <= kNear) flags[2] = 1;
-    if (m <= kTol) flags[0] = 1;
-    else diag[kMaxIters] = 0.0;  // the next storing pass records its own mismatch
+}
+
+// One Newton iteration (pass kind from the flags: with tangents until the mismatches are small, then
+// storing), or with final_pass the store pass after an iteration that converged without storing.
+template <int G>
+__global__ void __launch_bounds__(kShootThreads) shoot_pass_kernel(const srs_field *__restrict__ gfields, int nfields,
+                                                                   const srs_particle *__restrict__ part, Plan P,
+                                                                   Scratch W, double *__restrict__ X,
+                                                                   double *__restrict__ Bt, double *__restrict__ A,
+                                                                   int64_t stage_doubles, int final_pass) {
+  __shared__ PassShared<kShootThreads / G> sh;
+  const int conv = W.flags[0], near = W.flags[2], stored = W.flags[3];
+  if (final_pass) {
+    if (conv && !stored) shoot_pass<G, false>(sh, gfields, nfields, part, P, W, X, Bt, A, stage_doubles, true);
+  } else if (!conv) {
+    if (near) shoot_pass<G, false>(sh, gfields, nfields, part, P, W, X, Bt, A, stage_doubles, false);
+    else shoot_pass<G, true>(sh, gfields, nfields, part, P, W, X, Bt, A, stage_doubles, false);
   }
 }
 
@@ -381,7 +472,7 @@ __global__ void shoot_stats_kernel(const int *__restrict__ flags, const double *
   stats[0] = flags[0];
   stats[1] = it;
   stats[2] = it > 0 ? diag[(it < kMaxIters ? it : kMaxIters) - 1] : 0.0;
-  stats[3] = diag[kMaxIters];
+  stats[3] = it > 1 ? diag[(it < kMaxIters ? it : kMaxIters) - 2] : 0.0;
 }
 
 int lanes_for(int nfields) {
@@ -407,12 +498,6 @@ Plan make_plan(int64_t nfwd, int64_t nbwd, double dt, int steps_per_segment, int
   return P;
 }
 
-struct Scratch {
-  double *U, *F, *Phi, *Mc, *bc, *dstart, *diag;
-  int *flags;
-  double scale_pos, scale_vel;
-};
-
 Scratch carve(void *scratch, const Plan &P) {
   const size_t segs = (size_t)(P.sfp + P.sbp) + 1, chunks = (size_t)(P.sfp + P.sbp) / P.m + 1;
   Scratch s;
@@ -422,49 +507,40 @@ Scratch carve(void *scratch, const Plan &P) {
   s.Mc = s.Phi + 36 * segs;
   s.bc = s.Mc + 36 * chunks;
   s.dstart = s.bc + 6 * chunks;
-  s.diag = s.dstart + 6 * chunks;
-  s.flags = reinterpret_cast<int *>(s.diag + kMaxIters + 1);
+  s.Mp = s.dstart + 6 * chunks;
+  s.bp = s.Mp + 36 * chunks;
+  s.diag = s.bp + 6 * chunks;
+  s.rmax = s.diag + kMaxIters;
+  s.flags = reinterpret_cast<int *>(s.rmax + 1);
+  s.scale_pos = s.scale_vel = 1.0;
   return s;
 }
 
 template <int G>
-cudaError_t launch_fine(bool tan, int blocks, size_t smem, cudaStream_t s, const srs_field *d_fields, int nfields,
+cudaError_t launch_pass(int blocks, size_t smem, cudaStream_t s, const srs_field *d_fields, int nfields,
                         const srs_particle *d_particle, const Plan &P, const Scratch &W, double *d_x, double *d_b,
                         double *d_a, int64_t stage_doubles, int final_pass) {
-  if (tan) {
-    if (smem > 0)
-      if (cudaError_t e = cudaFuncSetAttribute(shoot_fine_kernel<G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem))
-        return e;
-    shoot_fine_kernel<G, true><<<blocks, kShootThreads, smem, s>>>(d_fields, nfields, d_particle, P, W.U, W.F, W.Phi,
-                                                                   W.Mc, W.bc, W.flags, W.diag + kMaxIters,
-                                                                   W.scale_pos, W.scale_vel, d_x, d_b, d_a,
-                                                                   stage_doubles, final_pass);
-  } else {
-    if (smem > 0)
-      if (cudaError_t e = cudaFuncSetAttribute(shoot_fine_kernel<G, false>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))
-        return e;
-    shoot_fine_kernel<G, false><<<blocks, kShootThreads, smem, s>>>(d_fields, nfields, d_particle, P, W.U, W.F,
-                                                                    W.Phi, W.Mc, W.bc, W.flags, W.diag + kMaxIters,
-                                                                    W.scale_pos, W.scale_vel, d_x, d_b, d_a,
-                                                                    stage_doubles, final_pass);
-  }
+  if (smem > 0)
+    if (cudaError_t e = cudaFuncSetAttribute(shoot_pass_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem))
+      return e;
+  shoot_pass_kernel<G><<<blocks, kShootThreads, smem, s>>>(d_fields, nfields, d_particle, P, W, d_x, d_b, d_a,
+                                                           stage_doubles, final_pass);
   return cudaGetLastError();
 }
 
-cudaError_t launch_fine_g(int G, bool tan, int blocks, size_t smem, cudaStream_t s, const srs_field *d_fields,
-                          int nfields, const srs_particle *d_particle, const Plan &P, const Scratch &W, double *d_x,
-                          double *d_b, double *d_a, int64_t stage_doubles, int final_pass) {
+cudaError_t launch_pass_g(int G, int blocks, size_t smem, cudaStream_t s, const srs_field *d_fields, int nfields,
+                          const srs_particle *d_particle, const Plan &P, const Scratch &W, double *d_x, double *d_b,
+                          double *d_a, int64_t stage_doubles, int final_pass) {
   switch (G) {
     case 8:
-      return launch_fine<8>(tan, blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a, stage_doubles,
+      return launch_pass<8>(blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a, stage_doubles,
                             final_pass);
     case 16:
-      return launch_fine<16>(tan, blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a, stage_doubles,
+      return launch_pass<16>(blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a, stage_doubles,
                              final_pass);
     case 32:
-      return launch_fine<32>(tan, blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a, stage_doubles,
+      return launch_pass<32>(blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a, stage_doubles,
                              final_pass);
     default:
       return cudaErrorInvalidValue;
@@ -484,7 +560,7 @@ int shoot_default_steps(int64_t nsteps) {
 size_t shoot_scratch_bytes(int64_t nfwd, int64_t nbwd, int steps_per_segment, int nfields) {
   const Plan P = make_plan(nfwd, nbwd, 1.0, steps_per_segment, nfields);
   const size_t segs = (size_t)(P.sfp + P.sbp) + 1, chunks = (size_t)(P.sfp + P.sbp) / P.m + 1;
-  return sizeof(double) * (segs * 48 + chunks * 48 + kMaxIters + 1) + 64;
+  return sizeof(double) * (segs * 48 + chunks * 90 + kMaxIters + 1) + 64;
 }
 
 cudaError_t launch_rk4_shoot(const srs_field *d_fields, int nfields, const srs_particle *d_particle,
@@ -505,23 +581,17 @@ cudaError_t launch_rk4_shoot(const srs_field *d_fields, int nfields, const srs_p
                          host_particle.beta0[1] * host_particle.beta0[1] +
                          host_particle.beta0[2] * host_particle.beta0[2]) * C;
   const double xs = fmax(fmax(fabs(host_particle.x0[0]), fabs(host_particle.x0[1])), fabs(host_particle.x0[2]));
-  const double scale_pos = fmax(fmax(xs, v0 * dt * (double)(P.mf > P.mb ? P.mf : P.mb)), 1e-300);
-  const double scale_vel = fmax(v0, 1e-300);
-  W.scale_pos = scale_pos;
-  W.scale_vel = scale_vel;
+  W.scale_pos = fmax(fmax(xs, v0 * dt * (double)(P.mf > P.mb ? P.mf : P.mb)), 1e-300);
+  W.scale_vel = fmax(v0, 1e-300);
   const size_t smem = sizeof(double) * (size_t)stage_doubles;
   const int G = lanes_for(nfields), blocks = segs / P.m;
-  shoot_init_kernel<<<(segs + 127) / 128, 128, 0, s>>>(P, d_particle, W.U, W.flags, W.diag);
-  for (int it = 0; it < iters; ++it) {
-    for (bool tan : {true, false})
-      if (cudaError_t e = launch_fine_g(G, tan, blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a,
-                                        stage_doubles, 0))
-        return e;
-    shoot_update_kernel<<<1, 1024, 0, s>>>(P, W.U, W.F, W.Phi, W.Mc, W.bc, W.dstart, W.flags, W.diag, scale_pos,
-                                           scale_vel);
-  }
+  shoot_init_kernel<<<(segs + 127) / 128, 128, 0, s>>>(P, d_particle, W);
+  for (int it = 0; it < iters; ++it)
+    if (cudaError_t e = launch_pass_g(G, blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a,
+                                      stage_doubles, 0))
+      return e;
   // converged after a pass with tangents: one more pass stores the points
-  if (cudaError_t e = launch_fine_g(G, false, blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a,
+  if (cudaError_t e = launch_pass_g(G, blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a,
                                     stage_doubles, 1))
     return e;
   if (d_stats) shoot_stats_kernel<<<1, 1, 0, s>>>(W.flags, W.diag, d_stats);

@@ -224,6 +224,9 @@ struct srs_sim {
   } cache;
   bool cache_enabled = true;
   int32_t traj_mode = SRS_TRAJ_AUTO;
+  // pinned staging of the caller's accumulator arrays (grow-only)
+  double *pinned = nullptr;
+  size_t pinned_doubles = 0;
   std::vector<Beam> beams;
   std::vector<double> weight_sums;
   std::map<std::string, size_t> beam_index;
@@ -236,6 +239,7 @@ struct srs_sim {
     if (cache.x) cudaFree(cache.x);
     if (cache.b) cudaFree(cache.b);
     if (cache.a) cudaFree(cache.a);
+    if (pinned) cudaFreeHost(pinned);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -446,8 +450,23 @@ struct srs_sim {
     DeviceBuffer dacc;
     SRS_CUDA(dacc.alloc(sizeof(double) * 2 * nout, stream));
     double *d_out = dacc.as<double>(), *d_comp = d_out + nout;
-    SRS_CUDA(cudaMemcpyAsync(d_out, out, sizeof(double) * nout, cudaMemcpyHostToDevice, stream));
-    SRS_CUDA(cudaMemcpyAsync(d_comp, comp, sizeof(double) * nout, cudaMemcpyHostToDevice, stream));
+    if ((size_t)(2 * nout) > pinned_doubles) {
+      if (pinned) SRS_CUDA(cudaFreeHost(pinned));
+      pinned = nullptr;
+      pinned_doubles = 0;
+      SRS_CUDA(cudaMallocHost(&pinned, sizeof(double) * 2 * nout));
+      pinned_doubles = 2 * nout;
+    }
+    // the caller's accumulators go up after the first batch's sums are queued: the host copies them
+    // into pinned memory while the GPU computes
+    bool uploaded = false;
+    auto upload = [&]() -> srs_status {
+      std::memcpy(pinned, out, sizeof(double) * nout);
+      std::memcpy(pinned + nout, comp, sizeof(double) * nout);
+      SRS_CUDA(cudaMemcpyAsync(d_out, pinned, sizeof(double) * 2 * nout, cudaMemcpyHostToDevice, stream));
+      uploaded = true;
+      return SRS_OK;
+    };
     const int bs = batch_size((int)ps.size());
     for (size_t b0 = 0; b0 < ps.size();) {
       // a batch shares t0 (particles of different beams may not)
@@ -466,12 +485,17 @@ struct srs_sim {
       SRS_CUDA(vals.alloc(sizeof(double) * (size_t)nout * np, stream));
       srs_beam_consts bc{ps[b0].q, ps[b0].current};
       if (srs_status st = sum(view, bc, vals.as<double>())) return st;
+      if (!uploaded)
+        if (srs_status st = upload()) return st;
       SRS_CUDA(accumulate_particles(vals.as<double>(), np, nout, weight, d_out, d_comp, stream));
       b0 = b1;
     }
-    SRS_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * nout, cudaMemcpyDeviceToHost, stream));
-    SRS_CUDA(cudaMemcpyAsync(comp, d_comp, sizeof(double) * nout, cudaMemcpyDeviceToHost, stream));
+    if (!uploaded)
+      if (srs_status st = upload()) return st;
+    SRS_CUDA(cudaMemcpyAsync(pinned, d_out, sizeof(double) * 2 * nout, cudaMemcpyDeviceToHost, stream));
     SRS_CUDA(cudaStreamSynchronize(stream));
+    std::memcpy(out, pinned, sizeof(double) * nout);
+    std::memcpy(comp, pinned + nout, sizeof(double) * nout);
     return SRS_OK;
   }
 };

@@ -120,7 +120,8 @@ def trajectory(fields, particles, ctstart, ctstop, t0, npoints, out=None):
 def trajectory_shoot(fields, particle, ctstart, ctstop, t0, npoints, steps_per_segment=0, max_iterations=0, out=None,
                      stats=None):
     """One particle's trajectory integrated parallel in time (srs_trajectory_shoot).  stats: optional
-    CUDA float64 tensor of 4 (converged, iterations, last update, segment defect)."""
+    CUDA float64 tensor of 4 (converged, iterations, largest segment mismatch of the last and of the
+    previous iteration)."""
     import torch
     dt, nf, nb = counts(ctstart, ctstop, t0, npoints)
     n = nf + nb
