@@ -112,7 +112,7 @@ __device__ inline V3 vadd_scaled(V3 a, double h, V3 b) { return v3(a.x + h * b.x
 // Copies every grid field's samples into the block's dynamic shared memory (the launcher sizes it to
 // the total when that fits) and points the prepared fields at the copies: the interpolation then
 // reads shared memory instead of global memory inside the serial RK4 chain.
-extern __shared__ double g_stage[];
+extern __shared__ __align__(16) double g_stage[];
 __device__ void stage_grids(const srs_field *sf, Prepared *sp, int nfields) {
   int64_t off = 0;
   for (int i = 0; i < nfields; ++i) {

@@ -32,6 +32,10 @@
 // rounds differently (~1e-15 m), not bit for bit; the FP64 drop-in path keeps the serial kernel.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
+#include <cuda_pipeline.h>
+
 #include "rk4_fields.cuh"
 #include "srs_internal.h"
 
@@ -43,6 +47,8 @@ constexpr int kMaxIters = 32;       // capacity of the per-iteration record
 constexpr int kDefaultIters = 8;
 constexpr double kTol = 4.440892098500626e-16;  // 2^-51 (~2 ulps of the speed): converged
 constexpr double kNear = 9.5367431640625e-07;   // 2^-20: keep the Jacobians, store the points
+constexpr int kChunkDoubles = 132;               // per-chunk data staged for the sweep
+constexpr int kMaxChunks = 192;                  // 192 x 132 doubles = 198 KB of shared memory
 
 struct Plan {
   int64_t mf, mb;         // steps of each chain
@@ -78,8 +84,8 @@ __device__ inline Seg seg_of(const Plan &P, int g) {
 // Device scratch of one integration.
 struct Scratch {
   double *U, *F, *Phi;     // per segment: start state, end state, Jacobian (row-major 6 x 6)
-  double *Mc, *bc, *dstart;  // per chunk: map (b without the boundary mismatch until the sweep), delta at its start
-  double *Mp, *bp;         // per chunk: the map up to its last segment's start
+  double *rec;             // per chunk, kChunkDoubles: the record the last block sweeps over (below)
+  double *dstart;          // per chunk: delta at its start
   double *diag;            // [it]: largest mismatch of iteration it (relative to the scales)
   double *rmax;            // this launch's largest interior mismatch (reset by the last block)
   int *flags;              // [0] converged, [1] iterations, [2] near, [3] the last pass stored, [4] ticket
@@ -172,6 +178,8 @@ __device__ __forceinline__ void shoot_pass(PassShared<kShootThreads / G> &sh, co
   __syncthreads();
   if (iter > 0 && !final_pass && t < 32) {  // one warp; lane i < 6 owns component i of delta
     const int i = lane < 6 ? lane : 0;
+    // (lane i reads sU[n + 1][i] before it writes it, and no lane reads a row that is written later in
+    // the same step, so the warp needs no barrier)
     double d = W.dstart[6 * c + i];
     for (int n = 0; n + 1 < M; ++n) {
       const Seg S = seg_of(P, g0 + n);
@@ -181,15 +189,19 @@ __device__ __forceinline__ void shoot_pass(PassShared<kShootThreads / G> &sh, co
       if (S.active && !S.last) {
         const double unew = sF[n][i] + dot6(&sPhi[n][6 * i], 1, dl, 1);  // = F_n exactly when delta_n = 0
         d = unew - sU[n + 1][i];
-        __syncwarp();
         if (lane < 6) sU[n + 1][i] = unew;
       }
-      __syncwarp();
     }
   }
   __syncthreads();
-  if (!final_pass)
+  // this chunk's record: [0, 36) M_c, [36, 42) b_c (without the boundary mismatch), [42, 84) the same
+  // up to the last segment's start, [84, 120) Phi of the last segment, [120, 126) its end state,
+  // [126, 132) the chunk's first start state
+  double *const rec = W.rec + (size_t)kChunkDoubles * c;
+  if (!final_pass) {
     for (int k = t; k < M * 6; k += blockDim.x) W.U[6 * g0 + k] = sU[k / 6][k % 6];
+    if (t < 6) rec[126 + t] = sU[0][t];
+  }
   if (stage_doubles > 0) stage_grids(sf, sp, nfields);  // (ends with a barrier)
 
   // (2) integrate
@@ -302,6 +314,7 @@ __device__ __forceinline__ void shoot_pass(PassShared<kShootThreads / G> &sh, co
   if (gl < 6) {
     const double fo[6] = {opos.x, opos.y, opos.z, ovel.x, ovel.y, ovel.z};
     W.F[6 * g + gl] = fo[gl];
+    if (grp == M - 1) rec[120 + gl] = fo[gl];
     const double r = link && grp + 1 < M ? fo[gl] - sU[grp + 1][gl] : 0.0;
     sR[grp][gl] = r;
     mis = fabs(r) / (gl < 3 ? W.scale_pos : W.scale_vel);
@@ -337,12 +350,13 @@ __device__ __forceinline__ void shoot_pass(PassShared<kShootThreads / G> &sh, co
     __syncthreads();
     cur ^= 1;
     if (n == M - 2) {  // the map up to the last segment's start
-      if (kTan && t < 36) W.Mp[36 * c + t] = sM[cur][t];
-      if (t >= 36 && t < 42) W.bp[6 * c + ti] = sB[cur][ti];
+      if (kTan && t < 36) rec[42 + t] = sM[cur][t];
+      if (t >= 36 && t < 42) rec[78 + ti] = sB[cur][ti];
     }
   }
-  if (kTan && t < 36) W.Mc[36 * c + t] = sM[cur][t];
-  if (t >= 36 && t < 42) W.bc[6 * c + ti] = sB[cur][ti];
+  if (kTan && t < 36) rec[t] = sM[cur][t];
+  if (t >= 36 && t < 42) rec[36 + ti] = sB[cur][ti];
+  if (kTan && t >= 64 && t < 100) rec[84 + t - 64] = sPhi[M - 1][t - 64];
 
   // the last block to finish decides and sweeps (the others' writes are fenced before their ticket)
   __threadfence();
@@ -352,20 +366,31 @@ __device__ __forceinline__ void shoot_pass(PassShared<kShootThreads / G> &sh, co
   if (!am_last) return;
   __threadfence();
   const int c0 = P.sfp / P.m, c1 = P.sbp / P.m, nch = c0 + c1;  // chunks of each chain
-  // the boundary mismatches: chunk c's last segment against chunk c + 1's first start state
+  // every chunk's record, copied into the block's dynamic shared memory (the grid samples' area: this
+  // block's integration is over) by asynchronous 16-byte copies, all in flight at once
+  double *const sm = g_stage;
+  {
+    const int n16 = nch * kChunkDoubles / 2;
+    for (int k = t; k < n16; k += blockDim.x) __pipeline_memcpy_async(sm + 2 * k, W.rec + 2 * k, 16);
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
+  }
+  __syncthreads();
+  // the boundary mismatches: chunk c's last segment against chunk c + 1's first start state, added to
+  // b_c (the block left them out)
   double bm = 0.0;
   for (int k = t; k < nch * 6; k += blockDim.x) {
-    const int cc = k / 6, i = k % 6, gl_ = cc * M + M - 1;
-    const Seg SL = seg_of(P, gl_);
+    const int cc = k / 6, i = k % 6;
+    const Seg SL = seg_of(P, cc * M + M - 1);
     if (SL.active && !SL.last) {
-      const double r = __ldcg(W.F + 6 * gl_ + i) - __ldcg(W.U + 6 * (gl_ + 1) + i);
-      W.bc[6 * cc + i] = __ldcg(W.bc + 6 * cc + i) + r;
+      double *const ch = sm + kChunkDoubles * cc;
+      const double r = ch[120 + i] - ch[kChunkDoubles + 126 + i];  // the next chunk's first start
+      ch[36 + i] = ch[36 + i] + r;
       bm = fmax(bm, fabs(r) / (i < 3 ? W.scale_pos : W.scale_vel));
     }
   }
   for (int o = 16; o > 0; o >>= 1) bm = fmax(bm, __shfl_xor_sync(full, bm, o));
   if (lane == 0) wred[t >> 5] = bm;
-  __threadfence();  // the chunk maps' boundary terms, read back through L2 by the sweep
   __syncthreads();
   if (t == 0) {
     double m = __longlong_as_double((long long)atomicAdd(reinterpret_cast<unsigned long long *>(W.rmax), 0ull));
@@ -381,69 +406,43 @@ __device__ __forceinline__ void shoot_pass(PassShared<kShootThreads / G> &sh, co
   }
   __syncthreads();
   if (done) return;
-  // carry delta across the chunk maps: warp w < 2 sweeps chain w, lane i < 6 owns component i; the
-  // maps are read three chunks ahead into registers (each of three buffers keeps its role, so a
-  // buffer's loads are consumed three chunks after they are issued)
+  // carry delta across the chunk maps: warp w < 2 sweeps chain w, lane i < 6 owning component i; delta
+  // at each chunk's start replaces that chunk's [126, 132) slot and goes to global memory for the next
+  // launch's expansion
   const int w = t >> 5;
   if (w < 2) {
     const int cn = w == 0 ? c0 : c1, first = w == 0 ? 0 : c0;
     const int i = lane < 6 ? lane : 0;
-    auto fetch = [&](int q, double *v) {
-      const int cg = first + q;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) v[k] = __ldcg(W.Mc + 36 * cg + 6 * i + k);
-      v[6] = __ldcg(W.bc + 6 * cg + i);
-    };
     double d = 0.0;
-    auto step = [&](int q, const double *v) {
-      if (lane < 6) W.dstart[6 * (first + q) + lane] = d;
+    for (int q = 0; q < cn; ++q) {
+      double *const ch = sm + kChunkDoubles * (first + q);
       double dl[6];
 #pragma unroll
       for (int k = 0; k < 6; ++k) dl[k] = __shfl_sync(full, d, k);
-      d = v[6] + dot6(v, 1, dl, 1);
-    };
-    double b0[7], b1[7], b2[7];
-    if (cn > 0) fetch(0, b0);
-    if (cn > 1) fetch(1, b1);
-    if (cn > 2) fetch(2, b2);
-    for (int q = 0; q < cn; q += 3) {
-      step(q, b0);
-      if (q + 3 < cn) fetch(q + 3, b0);
-      if (q + 1 < cn) step(q + 1, b1);
-      if (q + 4 < cn) fetch(q + 4, b1);
-      if (q + 2 < cn) step(q + 2, b2);
-      if (q + 5 < cn) fetch(q + 5, b2);
+      const double nd = ch[36 + i] + dot6(ch + 6 * i, 1, dl, 1);
+      if (lane < 6) {
+        W.dstart[6 * (first + q) + lane] = d;
+        ch[126 + lane] = d;
+      }
+      d = nd;
     }
   }
-  __threadfence_block();
   __syncthreads();
-  // every chunk, in parallel: delta at its last segment's start (the map up to there) and the next
-  // chunk's first start state U' = F_last + Phi_last delta_last (exactly F_last when delta_last = 0)
-  {
-    const int gi = t & 7, gb = lane & ~7, i = gi < 6 ? gi : 0;
-    for (int cb = 0; cb < nch; cb += kShootThreads / 8) {  // warp-uniform trip count
-      const int cg = cb + (t >> 3), gl_ = cg * M + M - 1;
-      const bool ok = cg < nch;
-      double dl[6], e[6], v[6];
-      double d0 = 0.0, dlast = 0.0;
-      if (ok) {
-        d0 = W.dstart[6 * cg + i];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) e[k] = __ldcg(W.Mp + 36 * cg + 6 * i + k);
-      }
-#pragma unroll
-      for (int k = 0; k < 6; ++k) dl[k] = __shfl_sync(full, d0, gb + k);
-      if (ok) dlast = __ldcg(W.bp + 6 * cg + i) + dot6(e, 1, dl, 1);
-#pragma unroll
-      for (int k = 0; k < 6; ++k) dl[k] = __shfl_sync(full, dlast, gb + k);
-      if (ok) {
-        const Seg SL = seg_of(P, gl_);
-        if (gi < 6 && SL.active && !SL.last) {
-#pragma unroll
-          for (int k = 0; k < 6; ++k) v[k] = __ldcg(W.Phi + 36 * gl_ + 6 * i + k);
-          W.U[6 * (gl_ + 1) + i] = __ldcg(W.F + 6 * gl_ + i) + dot6(v, 1, dl, 1);
-        }
-      }
+  // every chunk, in parallel: delta at its last segment's start (the map up to there; into the
+  // chunk's [78, 84) slot), then the next chunk's first start state U' = F_last + Phi_last delta_last
+  // (exactly F_last when delta_last = 0)
+  for (int k = t; k < nch * 6; k += blockDim.x) {
+    double *const ch = sm + kChunkDoubles * (k / 6);
+    const int i = k % 6;
+    ch[78 + i] = ch[78 + i] + dot6(ch + 42 + 6 * i, 1, ch + 126, 1);
+  }
+  __syncthreads();
+  for (int k = t; k < nch * 6; k += blockDim.x) {
+    const int cc = k / 6, i = k % 6, gl_ = cc * M + M - 1;
+    const Seg SL = seg_of(P, gl_);
+    if (SL.active && !SL.last) {
+      const double *const ch = sm + kChunkDoubles * cc;
+      W.U[6 * (gl_ + 1) + i] = ch[120 + i] + dot6(ch + 84 + 6 * i, 1, ch + 78, 1);
     }
   }
 }
@@ -487,6 +486,9 @@ Plan make_plan(int64_t nfwd, int64_t nbwd, double dt, int steps_per_segment, int
   P.mb = nbwd;
   P.L = steps_per_segment > 0 ? steps_per_segment : shoot_default_steps(P.mf + P.mb);
   P.m = kShootThreads / lanes_for(nfields);
+  // at most kMaxChunks chunks (their data are staged in shared memory for the sweep): longer segments
+  // than asked for if needed
+  while (((P.mf + P.L - 1) / P.L + (P.mb + P.L - 1) / P.L) > (int64_t)(kMaxChunks - 2) * P.m) P.L *= 2;
   P.sf = (int)((P.mf + P.L - 1) / P.L);
   P.sb = (int)((P.mb + P.L - 1) / P.L);
   P.sfp = (P.sf + P.m - 1) / P.m * P.m;
@@ -504,12 +506,9 @@ Scratch carve(void *scratch, const Plan &P) {
   s.U = static_cast<double *>(scratch);
   s.F = s.U + 6 * segs;
   s.Phi = s.F + 6 * segs;
-  s.Mc = s.Phi + 36 * segs;
-  s.bc = s.Mc + 36 * chunks;
-  s.dstart = s.bc + 6 * chunks;
-  s.Mp = s.dstart + 6 * chunks;
-  s.bp = s.Mp + 36 * chunks;
-  s.diag = s.bp + 6 * chunks;
+  s.rec = s.Phi + 36 * segs;
+  s.dstart = s.rec + kChunkDoubles * chunks;
+  s.diag = s.dstart + 6 * chunks;
   s.rmax = s.diag + kMaxIters;
   s.flags = reinterpret_cast<int *>(s.rmax + 1);
   s.scale_pos = s.scale_vel = 1.0;
@@ -560,7 +559,7 @@ int shoot_default_steps(int64_t nsteps) {
 size_t shoot_scratch_bytes(int64_t nfwd, int64_t nbwd, int steps_per_segment, int nfields) {
   const Plan P = make_plan(nfwd, nbwd, 1.0, steps_per_segment, nfields);
   const size_t segs = (size_t)(P.sfp + P.sbp) + 1, chunks = (size_t)(P.sfp + P.sbp) / P.m + 1;
-  return sizeof(double) * (segs * 48 + chunks * 90 + kMaxIters + 1) + 64;
+  return sizeof(double) * (segs * 48 + chunks * (kChunkDoubles + 6) + kMaxIters + 1) + 64;
 }
 
 cudaError_t launch_rk4_shoot(const srs_field *d_fields, int nfields, const srs_particle *d_particle,
@@ -583,7 +582,8 @@ cudaError_t launch_rk4_shoot(const srs_field *d_fields, int nfields, const srs_p
   const double xs = fmax(fmax(fabs(host_particle.x0[0]), fabs(host_particle.x0[1])), fabs(host_particle.x0[2]));
   W.scale_pos = fmax(fmax(xs, v0 * dt * (double)(P.mf > P.mb ? P.mf : P.mb)), 1e-300);
   W.scale_vel = fmax(v0, 1e-300);
-  const size_t smem = sizeof(double) * (size_t)stage_doubles;
+  // dynamic shared memory: the grid samples during the integration, the chunk maps in the sweep
+  const size_t smem = sizeof(double) * (size_t)std::max<int64_t>(stage_doubles, (int64_t)(segs / P.m) * kChunkDoubles);
   const int G = lanes_for(nfields), blocks = segs / P.m;
   shoot_init_kernel<<<(segs + 127) / 128, 128, 0, s>>>(P, d_particle, W);
   for (int it = 0; it < iters; ++it)
