@@ -916,14 +916,19 @@ srs_status srs_energy_grid(int64_t n, double e0, double e1, double *out) {
 
 static void rect_emit(int n1, int n2, V3 start, V3 v1, V3 v2, double s1, double s2, V3 nv, double *xyz, double *x12,
                       double nrm[3], srs_grid2d *grid) {
-  const size_t np = (size_t)(n1 * n2);
-  for (size_t i = 0; i < np; ++i) {
-    const int i1 = (int)(i / n2), i2 = (int)(i % n2);
-    V3 p = start + v1 * (double)i1 + v2 * (double)i2;  // TSurfacePoints_Rectangle.cc:222-230
-    if (xyz) put(xyz + 3 * i, p);
-    if (x12) {
-      x12[2 * i] = s1 * i1 - mag(v1) * (n1 - 1) / 2.;      // :244-251
-      x12[2 * i + 1] = s2 * i2 - mag(v2) * (n2 - 1) / 2.;  // :252-259
+  // the offsets of GetX1 / GetX2 (:244-259) do not depend on the point: computed once, same values
+  const double off1 = mag(v1) * (n1 - 1) / 2., off2 = mag(v2) * (n2 - 1) / 2.;
+  size_t i = 0;
+  for (int i1 = 0; i1 < n1; ++i1) {
+    const V3 row = start + v1 * (double)i1;
+    const double a1 = s1 * i1 - off1;
+    for (int i2 = 0; i2 < n2; ++i2, ++i) {
+      const V3 p = row + v2 * (double)i2;  // TSurfacePoints_Rectangle.cc:222-230: start + v1 i1 + v2 i2
+      if (xyz) put(xyz + 3 * i, p);
+      if (x12) {
+        x12[2 * i] = a1;
+        x12[2 * i + 1] = s2 * i2 - off2;
+      }
     }
   }
   if (nrm) put(nrm, unit(nv));  // TSurfacePoint normalises the normal again
