@@ -18,6 +18,7 @@ import math
 import numpy as np
 
 from . import _lib
+from . import aggregate as _agg
 from ._lib import check, dptr, lib, v3
 
 _ZERO3 = (0.0, 0.0, 0.0)
@@ -56,6 +57,9 @@ class sr:  # noqa: N801  (the reference's type name)
         self._h = h
         self._nthreads_global = 2
         self._precision = _lib.FP64
+        self._spectrum_sum = _agg.SpectrumSum()
+        self._flux_sum = _agg.ScalarSum()
+        self._pd_sum = _agg.ScalarSum()
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -611,6 +615,89 @@ class sr:  # noqa: N801  (the reference's type name)
         out = C.c_double()
         check(lib.srs_sim_calculate_total_power(self._h, C.byref(out)))
         return out.value
+
+
+def _spectrum_from_list(spectrum):
+    """OSCARSSR_GetSpectrumFromList (OSCARSSR_Python.cc:2113-2143): [[E, flux], ...]."""
+    rows = []
+    for p in spectrum:
+        if len(p) != 2:
+            _bad_entry()
+        rows.append((float(p[0]), float(p[1])))
+    a = np.array(rows, dtype=np.float64).reshape(-1, 2)
+    return a[:, 0], a[:, 1]
+
+
+def _scalars_from_list(points):
+    """OSCARSSR_GetT3DScalarContainerFromList (OSCARSSR_Python.cc:2151-2180): [[[x, y, z], v], ...];
+    a position that is not three numbers is a length error ("number of elements not 3")."""
+    xyz, vals = [], []
+    for p in points:
+        if len(p) != 2:
+            _bad_entry()
+        if len(p[0]) != 3:
+            raise ValueError("number of elements not 3")
+        xyz.append([float(c) for c in p[0]])
+        vals.append(float(p[1]))
+    return np.array(xyz, dtype=np.float64).reshape(-1, 3), np.array(vals, dtype=np.float64)
+
+
+def _bad_entry():
+    raise ValueError("each entry must be a list of 2 elements")
+
+
+def _aggregation_methods():
+    """The reference's running sums and file averages (OSCARSSR_Python.cc:3252-3572), attached to sr."""
+
+    def add_to_spectrum(self, spectrum, weight=1):
+        """Add weight * spectrum to the object's running spectrum (compensated sum)."""
+        if len(spectrum) < 1:
+            raise ValueError("No points in spectrum.")
+        e, f = _spectrum_from_list(spectrum)
+        self._spectrum_sum.add(e, f, float(weight))
+
+    def get_spectrum(self):
+        return self._spectrum_sum.as_list()
+
+    def add_to_flux(self, flux, weight=1):
+        """Add weight * flux (a map [[[x, y, z], v], ...]) to the object's running flux."""
+        if len(flux) < 1:
+            raise ValueError("No points in flux.")
+        xyz, v = _scalars_from_list(flux)
+        self._flux_sum.add(xyz, v, float(weight))
+
+    def get_flux(self):
+        return self._flux_sum.as_list()
+
+    def add_to_power_density(self, power_density, weight=1):
+        """Add weight * power_density to the object's running power density."""
+        if len(power_density) < 1:
+            raise ValueError("No points in flux.")  # the reference's message
+        xyz, v = _scalars_from_list(power_density)
+        self._pd_sum.add(xyz, v, float(weight))
+
+    def get_power_density(self):
+        return self._pd_sum.as_list()
+
+    def average_spectra(self, ifiles=None, bifiles=None, ofile="", bofile=""):
+        """The point-by-point average of spectrum files (text; binary input gives an empty result,
+        as in the reference)."""
+        return _agg.average_spectra(ifiles, bifiles, ofile, bofile)
+
+    def average_flux(self, ifiles=None, bifiles=None, ofile="", bofile="", dim=2):
+        """The point-by-point average of flux-map files (text or binary, dim 2 or 3)."""
+        return _agg.average_scalars(ifiles, bifiles, ofile, bofile, dim)
+
+    def average_power_density(self, ifiles=None, bifiles=None, ofile="", bofile="", dim=2):
+        """The point-by-point average of power-density files (text or binary, dim 2 or 3)."""
+        return _agg.average_scalars(ifiles, bifiles, ofile, bofile, dim)
+
+    for fn in (add_to_spectrum, get_spectrum, add_to_flux, get_flux, add_to_power_density, get_power_density,
+               average_spectra, average_flux, average_power_density):
+        setattr(sr, fn.__name__, fn)
+
+
+_aggregation_methods()
 
 
 def rectangle_points(npoints, plane="", width=None, x0x1x2=None, rotations=None, translation=None, normal=0):

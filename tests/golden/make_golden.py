@@ -294,9 +294,109 @@ def quirks():
         json.dump(res, fh, indent=1)
 
 
+def aggregate():
+    """Running sums (add_to_* / get_*) and file averages (average_*) of the reference's containers
+    (OSCARSSR_Python.cc:3252-3572, TSpectrumContainer.cc:159-175, 318-395, T3DScalarContainer.cc:31-320)
+    on seeded synthetic spectra and maps: values spanning many magnitudes so the compensated sums
+    matter, weights, dim 2 and 3, text and binary files."""
+    rng = np.random.default_rng(5)
+    out = {}
+    o = new_sr()
+    ne = 37
+    e = np.linspace(100.0, 1000.0, ne)
+    spectra = [(rng.lognormal(0.0, 6.0, ne) * rng.choice([1.0, 1e-9, 1e9], ne)).tolist() for _ in range(4)]
+    weights = [0.25, 1.0 / 3.0, 0.7, 1e-3]
+    for k, (sp, w) in enumerate(zip(spectra, weights)):
+        o.add_to_spectrum(spectrum=[[float(a), float(b)] for a, b in zip(e, sp)], weight=w)
+    got = o.get_spectrum()
+    out["spec_in"] = np.array(spectra)
+    out["spec_e"] = e
+    out["spec_w"] = np.array(weights)
+    out["spec_sum"] = np.array(got)
+    npt = 23
+    xyz = rng.normal(0.0, 0.01, (npt, 3))
+    maps = [(rng.lognormal(0.0, 5.0, npt) * rng.choice([1.0, 1e-8, 1e8], npt)).tolist() for _ in range(3)]
+    mw = [0.5, 1.0 / 7.0, 2.0]
+    for fn, getter, tag in ((o.add_to_flux, o.get_flux, "flux"), (o.add_to_power_density, o.get_power_density, "pd")):
+        for m, w in zip(maps, mw):
+            kw = {"flux" if tag == "flux" else "power_density": [[list(map(float, x)), float(v)] for x, v in zip(xyz, m)],
+                  "weight": w}
+            fn(**kw)
+        r = getter()
+        out[f"{tag}_xyz"] = np.array([q[0] for q in r])
+        out[f"{tag}_sum"] = np.array([q[1] for q in r])
+    out["map_in"] = np.array(maps)
+    out["map_xyz"] = xyz
+    out["map_w"] = np.array(mw)
+    # file averages: text spectra (the reference's own %e format, and full precision), dim-2 and
+    # dim-3 text maps, dim-2 and dim-3 binary maps, the outputs the reference writes
+    with tempfile.TemporaryDirectory() as td:
+        files = []
+        for k in range(3):
+            path = os.path.join(td, f"s{k}.txt")
+            with open(path, "w") as fh:
+                for a, b in zip(e, spectra[k]):
+                    fh.write(f"{a:.6e} {b:.6e}\n" if k != 1 else f"{float(a)!r} {float(b)!r}\n")
+            files.append(path)
+        # the first file without a trailing newline: the reference drops its last point
+        path = os.path.join(td, "s_nonl.txt")
+        with open(path, "w") as fh:
+            fh.write("\n".join(f"{a:.6e} {b:.6e}" for a, b in zip(e, spectra[3])))
+        files_nonl = [path, files[0]]
+        oav = new_sr()
+        ofile = os.path.join(td, "avg.txt")
+        r = oav.average_spectra(ifiles=[f.encode() for f in files], ofile=ofile)
+        out["avg_spec"] = np.array(r)
+        out["avg_spec_ofile"] = np.frombuffer(open(ofile, "rb").read(), dtype=np.uint8)
+        r = oav.average_spectra(ifiles=[f.encode() for f in files_nonl])
+        out["avg_spec_nonl"] = np.array(r)
+        out["avg_spec_binary_len"] = len(oav.average_spectra(bifiles=[f.encode() for f in files]))
+        for k in range(3):
+            with open(files[k]) as fh:
+                out[f"spec_file{k}"] = np.frombuffer(fh.read().encode(), dtype=np.uint8)
+        with open(files_nonl[0]) as fh:
+            out["spec_file_nonl"] = np.frombuffer(fh.read().encode(), dtype=np.uint8)
+        for dim in (2, 3):
+            tf, bf = [], []
+            for k in range(3):
+                tp, bp = os.path.join(td, f"m{dim}_{k}.txt"), os.path.join(td, f"m{dim}_{k}.bin")
+                with open(tp, "w") as fh:
+                    for x, v in zip(xyz, maps[k]):
+                        cols = list(x[:dim]) + [v]
+                        fh.write(" ".join(f"{c:.6e}" for c in cols) + "\n")
+                rows = np.column_stack([xyz[:, :dim], maps[k]]).astype(np.float64)
+                rows.tofile(bp)
+                tf.append(tp)
+                bf.append(bp)
+                out[f"map{dim}_text{k}"] = np.frombuffer(open(tp, "rb").read(), dtype=np.uint8)
+                out[f"map{dim}_bin{k}"] = np.frombuffer(open(bp, "rb").read(), dtype=np.uint8)
+            of_t, of_b = os.path.join(td, "avgm.txt"), os.path.join(td, "avgm.bin")
+            r = oav.average_flux(ifiles=[f.encode() for f in tf], dim=dim, ofile=of_t, bofile=of_b)
+            out[f"avg_flux{dim}_text"] = np.array([[*q[0], q[1]] for q in r])
+            out[f"avg_flux{dim}_ofile"] = np.frombuffer(open(of_t, "rb").read(), dtype=np.uint8)
+            out[f"avg_flux{dim}_bofile"] = np.frombuffer(open(of_b, "rb").read(), dtype=np.uint8)
+            r = oav.average_power_density(bifiles=[f.encode() for f in bf], dim=dim)
+            out[f"avg_pd{dim}_binary"] = np.array([[*q[0], q[1]] for q in r])
+    errs = {}
+    for name, call in (("both_kinds", lambda: oav.average_spectra(ifiles=[b"a"], bifiles=[b"b"])),
+                       ("no_files", lambda: oav.average_spectra()),
+                       ("no_files_flux", lambda: oav.average_flux()),
+                       ("empty_spectrum", lambda: o.add_to_spectrum(spectrum=[])),
+                       ("empty_flux", lambda: o.add_to_flux(flux=[])),
+                       ("empty_pd", lambda: o.add_to_power_density(power_density=[]))):
+        try:
+            call()
+            errs[name] = None
+        except ValueError as exc:
+            errs[name] = str(exc)
+    with open(os.path.join(HERE, "aggregate_errors.json"), "w") as fh:
+        json.dump(errs, fh, indent=1)
+    save("aggregate.npz", **out)
+
+
 if __name__ == "__main__":
     parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "beam32", "points", "grid", "adjoint",
-                             "quirks"]
+                             "quirks", "aggregate"]
     if "cfg0" in parts:
         e1 = cfg0()
         print("E1 (first-harmonic peak of the config-0 spectrum):", repr(e1))
@@ -307,6 +407,6 @@ if __name__ == "__main__":
     for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("beam32", beam32), ("points", points_surface),
                      ("grid", grid),
                      ("adjoint", adjoint),
-                     ("quirks", quirks)):
+                     ("quirks", quirks), ("aggregate", aggregate)):
         if name in parts:
             fn()
