@@ -324,11 +324,33 @@ srs_status srs_sim_add_bfield_gaussian(srs_sim *sim, const double bfield[3], con
                                        const double rotations[3], const double translation[3]);
 srs_status srs_sim_add_bfield_uniform(srs_sim *sim, const double bfield[3], const double width[3],
                                       const double rotations[3], const double translation[3]);
-/* OSCARS-format field map file (TField3D_Grid::ReadFile): scale[0..2] step scaling, [3..5] field
- * scaling (nscale may be 0). */
+/* Field map file (OSCARSSR::AddMagneticField, OSCARSSR.cc:68-90; TField3D_Grid.cc:25-45) in one of
+ * the reference's formats (case-insensitive): "OSCARS" (regular grid; scale[0..2] step scaling,
+ * [3..5] field scaling), "OSCARS1D <columns>" (irregular samples along one axis, columns named
+ * X|Y|Z and Bx|By|Bz (or Ex.., Fx..) in file order, scale factors per column, regridded at 10000
+ * points per metre), "SRW" or "SPECTRA" (no scaling).  nscale may be 0. */
 srs_status srs_sim_add_bfield_file(srs_sim *sim, const char *path, const char *format,
                                    const double rotations[3], const double translation[3],
                                    const double *scale, int32_t nscale);
+/* Field map interpolated between OSCARS-format files (add_bfield_interpolated,
+ * OSCARSSR_Python.cc:419-510; TField3D_Grid.cc:1150-1420): nmap pairs (parameter, path), identical
+ * headers, the map at `parameter` by linear interpolation between the two files around it.  At
+ * exactly the smallest mapping parameter the reference's result is NaN, reproduced. */
+srs_status srs_sim_add_bfield_interpolated(srs_sim *sim, const double *parameters, const char *const *paths,
+                                           int32_t nmap, const char *format, double parameter,
+                                           const double rotations[3], const double translation[3],
+                                           const double *scale, int32_t nscale);
+/* The same readers without a simulation object (host only, no GPU): the grid descriptor (its data
+ * pointer NULL) and the rotated samples, 3 doubles each, into data when *ndata is large enough;
+ * *ndata returns the number of doubles.  No reference counterpart (the reference reads inside
+ * add_bfield_file / add_bfield_interpolated). */
+srs_status srs_read_field_file(const char *path, const char *format, const double rotations[3],
+                               const double translation[3], const double *scale, int32_t nscale, srs_field *out,
+                               double *data, int64_t *ndata);
+srs_status srs_read_field_interpolated(const double *parameters, const char *const *paths, int32_t nmap,
+                                       const char *format, double parameter, const double rotations[3],
+                                       const double translation[3], const double *scale, int32_t nscale,
+                                       srs_field *out, double *data, int64_t *ndata);
 /* Field map given as arrays (same meaning as the file's header and body). */
 srs_status srs_sim_add_bfield_grid(srs_sim *sim, const double start[3], const double step[3],
                                    const int64_t n[3], const double *data, const double rotations[3],

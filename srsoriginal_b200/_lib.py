@@ -101,6 +101,12 @@ def _load():
         "srs_sim_add_bfield_gaussian": (S, [P, _D, _D, _D, _D]),
         "srs_sim_add_bfield_uniform": (S, [P, _D, _D, _D, _D]),
         "srs_sim_add_bfield_file": (S, [P, C.c_char_p, C.c_char_p, _D, _D, _D, C.c_int32]),
+        "srs_sim_add_bfield_interpolated": (S, [P, _D, C.POINTER(C.c_char_p), C.c_int32, C.c_char_p, C.c_double,
+                                                _D, _D, _D, C.c_int32]),
+        "srs_read_field_file": (S, [C.c_char_p, C.c_char_p, _D, _D, _D, C.c_int32, C.POINTER(Field), _D,
+                                    C.POINTER(C.c_int64)]),
+        "srs_read_field_interpolated": (S, [_D, C.POINTER(C.c_char_p), C.c_int32, C.c_char_p, C.c_double, _D, _D,
+                                            _D, C.c_int32, C.POINTER(Field), _D, C.POINTER(C.c_int64)]),
         "srs_sim_add_bfield_grid": (S, [P, _D, _D, C.POINTER(C.c_int64), _D, _D, _D]),
         "srs_sim_clear_bfields": (S, [P]),
         "srs_sim_set_trajectory_cache": (S, [P, C.c_int32]),
@@ -160,7 +166,7 @@ EXPORTED = (
     "srs_sim_set_ctstartstop srs_sim_set_npoints_trajectory srs_sim_get_ctstartstop "
     "srs_sim_get_npoints_trajectory srs_sim_set_nthreads_global srs_sim_set_gpu_global "
     "srs_sim_add_bfield_undulator srs_sim_add_bfield_gaussian srs_sim_add_bfield_uniform "
-    "srs_sim_add_bfield_file srs_sim_add_bfield_grid srs_sim_clear_bfields srs_sim_get_nfields "
+    "srs_read_field_file srs_read_field_interpolated srs_sim_add_bfield_interpolated srs_sim_add_bfield_file srs_sim_add_bfield_grid srs_sim_clear_bfields srs_sim_get_nfields "
     "srs_sim_set_trajectory_cache srs_sim_set_trajectory_mode "
     "srs_sim_get_bfield srs_sim_set_field_grid_data srs_sim_add_particle_beam "
     "srs_sim_clear_particle_beams srs_sim_get_nparticle_beams srs_sim_set_new_particle "

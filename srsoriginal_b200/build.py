@@ -32,6 +32,7 @@ SOURCES = [
     ("adjoint.cu", True),
     ("capi.cu", True),
     ("sim.cpp", True),
+    ("field_files.cpp", True),
     ("peaks.cu", False),
 ]
 

@@ -138,60 +138,6 @@ struct Beam {
   }
 };
 
-// ---------------------------------------------------------------- OSCARS grid file (TField3D_Grid::ReadFile)
-srs_status read_oscars_grid(const std::string &path, const double rot3[3], const double trans[3], const double *scale,
-                            int nscale, srs_field &f, std::vector<double> &data) {
-  std::ifstream fi(path);
-  if (!fi) return fail(SRS_ERR_IO, "Could not import magnetic field.  Check 'ifile' and 'iformat' are correct");
-  std::string L;
-  std::getline(fi, L);  // comment line
-  double hv[9];
-  for (int k = 0; k < 9; ++k) {
-    if (!std::getline(fi, L)) return fail(SRS_ERR_IO, "cannot read header value");
-    std::istringstream S(L);
-    S >> hv[k];
-    if (S.fail()) return fail(SRS_ERR_IO, "cannot read header value");
-  }
-  const int NX = (int)hv[2], NY = (int)hv[5], NZ = (int)hv[8];
-  const double XStepIN = hv[1], YStepIN = hv[4], ZStepIN = hv[7];
-  const double XStep = nscale > 0 ? XStepIN * scale[0] : XStepIN;
-  const double YStep = nscale > 1 ? YStepIN * scale[1] : YStepIN;
-  const double ZStep = nscale > 2 ? ZStepIN * scale[2] : ZStepIN;
-  const double FxS = nscale > 3 ? scale[3] : 1, FyS = nscale > 4 ? scale[4] : 1, FzS = nscale > 5 ? scale[5] : 1;
-  const double MiddleX = hv[0] + XStepIN * (NX - 1) / 2., XStart = MiddleX - XStep * (NX - 1) / 2.;
-  const double MiddleY = hv[3] + YStepIN * (NY - 1) / 2., YStart = MiddleY - YStep * (NY - 1) / 2.;
-  const double MiddleZ = hv[6] + ZStepIN * (NZ - 1) / 2., ZStart = MiddleZ - ZStep * (NZ - 1) / 2.;
-  if (NX < 1 || NY < 1 || NZ < 1) return fail(SRS_ERR_RANGE, "invalid number of points in at least one dimension");
-  if (NX == 1 && NY == 1 && NZ == 1) return fail(SRS_ERR_RANGE, "invalid dimensions");
-  const size_t n = (size_t)NX * NY * NZ;
-  data.resize(3 * n);
-  std::istringstream S;
-  for (size_t i = 0; i < n; ++i) {
-    std::getline(fi, L);
-    if (fi.eof() && L.empty()) return fail(SRS_ERR_IO, "error reading file.  Check format");
-    double fx, fy, fz;
-    S.clear();
-    S.str(L);
-    S >> fx >> fy >> fz;
-    if (S.fail()) return fail(SRS_ERR_IO, "error reading file.  Check format");
-    if (FxS != 1) fx *= FxS;
-    if (FyS != 1) fy *= FyS;
-    if (FzS != 1) fz *= FzS;
-    V3 F = rot(v3(fx, fy, fz), rot3);
-    data[3 * i] = F.x;
-    data[3 * i + 1] = F.y;
-    data[3 * i + 2] = F.z;
-  }
-  std::memset(&f, 0, sizeof f);
-  f.kind = SRS_FIELD_GRID;
-  f.start[0] = XStart; f.start[1] = YStart; f.start[2] = ZStart;
-  f.step[0] = XStep; f.step[1] = YStep; f.step[2] = ZStep;
-  f.n[0] = NX; f.n[1] = NY; f.n[2] = NZ;
-  std::memcpy(f.rotations, rot3, sizeof(double) * 3);
-  std::memcpy(f.translation, trans, sizeof(double) * 3);
-  return SRS_OK;
-}
-
 }  // namespace
 }  // namespace srs
 
@@ -601,11 +547,69 @@ srs_status srs_sim_add_bfield_file(srs_sim *sim, const char *path, const char *f
                                    const double translation[3], const double *scale, int32_t nscale) {
   SIM_GUARD(sim);
   if (!path || !format || !*path || !*format) return fail(SRS_ERR_INVALID, "'ifile' or 'iformat' is blank");
-  if (upper(format) != "OSCARS")
-    return fail(SRS_ERR_INVALID, "Could not import magnetic field.  Check 'ifile' and 'iformat' are correct");
   srs_field f;
   std::vector<double> data;
-  if (srs_status st = read_oscars_grid(path, rotations, translation, scale, nscale, f, data)) return st;
+  if (srs_status st = read_field_file(path, format, rotations, translation, scale, nscale, f, data)) return st;
+  return sim->add_field(f, std::move(data));
+}
+
+srs_status srs_read_field_file(const char *path, const char *format, const double rotations[3],
+                               const double translation[3], const double *scale, int32_t nscale, srs_field *out,
+                               double *data, int64_t *ndata) {
+  clear_error();
+  if (!path || !format || !*path || !*format) return fail(SRS_ERR_INVALID, "'ifile' or 'iformat' is blank");
+  if (!out || !ndata || !rotations || !translation) return fail(SRS_ERR_INVALID, "NULL argument");
+  srs_field f;
+  std::vector<double> d;
+  if (srs_status st = read_field_file(path, format, rotations, translation, scale, nscale, f, d)) return st;
+  *out = f;
+  out->data = nullptr;
+  if (data && *ndata >= (int64_t)d.size()) std::memcpy(data, d.data(), sizeof(double) * d.size());
+  *ndata = (int64_t)d.size();
+  return SRS_OK;
+}
+
+srs_status srs_read_field_interpolated(const double *parameters, const char *const *paths, int32_t nmap,
+                                       const char *format, double parameter, const double rotations[3],
+                                       const double translation[3], const double *scale, int32_t nscale,
+                                       srs_field *out, double *data, int64_t *ndata) {
+  clear_error();
+  if (!format || !*format) return fail(SRS_ERR_INVALID, "'iformat' is blank");
+  if (!out || !ndata || !rotations || !translation || nmap < 0 || (nmap > 0 && (!parameters || !paths)))
+    return fail(SRS_ERR_INVALID, "NULL argument");
+  std::vector<std::pair<double, std::string>> mapping;
+  for (int i = 0; i < nmap; ++i) {
+    if (!paths[i]) return fail(SRS_ERR_INVALID, "Incorrect format in 'mapping'");
+    mapping.emplace_back(parameters[i], paths[i]);
+  }
+  srs_field f;
+  std::vector<double> d;
+  if (srs_status st = read_field_interpolated(mapping, format, parameter, rotations, translation, scale, nscale, f, d))
+    return st;
+  *out = f;
+  out->data = nullptr;
+  if (data && *ndata >= (int64_t)d.size()) std::memcpy(data, d.data(), sizeof(double) * d.size());
+  *ndata = (int64_t)d.size();
+  return SRS_OK;
+}
+
+srs_status srs_sim_add_bfield_interpolated(srs_sim *sim, const double *parameters, const char *const *paths,
+                                           int32_t nmap, const char *format, double parameter,
+                                           const double rotations[3], const double translation[3],
+                                           const double *scale, int32_t nscale) {
+  SIM_GUARD(sim);
+  if (!format || !*format) return fail(SRS_ERR_INVALID, "'iformat' is blank");
+  if (nmap < 0 || (nmap > 0 && (!parameters || !paths))) return fail(SRS_ERR_INVALID, "Incorrect format in 'mapping'");
+  std::vector<std::pair<double, std::string>> mapping;
+  for (int i = 0; i < nmap; ++i) {
+    if (!paths[i]) return fail(SRS_ERR_INVALID, "Incorrect format in 'mapping'");
+    mapping.emplace_back(parameters[i], paths[i]);
+  }
+  srs_field f;
+  std::vector<double> data;
+  if (srs_status st = read_field_interpolated(mapping, format, parameter, rotations, translation, scale, nscale, f,
+                                              data))
+    return st;
   return sim->add_field(f, std::move(data));
 }
 

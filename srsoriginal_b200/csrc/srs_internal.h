@@ -5,6 +5,8 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "../../include/srs_b200.h"
 
@@ -52,6 +54,14 @@ struct TrajSpec {
   int64_t nfwd, nbwd;
   double *x, *beta, *aoc;  // 3 * (nfwd + nbwd) doubles each, [component][point]
 };
+
+// ---- field maps from files (field_files.cpp): the grid descriptor and its samples (host) ----
+srs_status read_field_file(const std::string &path, const std::string &format, const double rot[3],
+                           const double trans[3], const double *scale, int nscale, srs_field &f,
+                           std::vector<double> &data);
+srs_status read_field_interpolated(std::vector<std::pair<double, std::string>> mapping, const std::string &format,
+                                   double parameter, const double rot[3], const double trans[3],
+                                   const double *scale, int nscale, srs_field &f, std::vector<double> &data);
 
 // ---- kernel launchers ----
 // Grid samples (doubles) to stage in shared memory for these fields (HOST array): their total, or 0

@@ -157,6 +157,30 @@ class sr:  # noqa: N801  (the reference's type name)
                 raise ValueError(msg)
             raise ValueError("Could not import magnetic field.  Check 'ifile' and 'iformat' are correct")
 
+    def add_bfield_interpolated(self, mapping, iformat, parameter, rotations=None, translation=None, scale=None):
+        """A field map interpolated between files by a parameter (e.g. an undulator gap):
+        mapping = [[parameter value, file name], ...] of OSCARS-format files with the same grid
+        (OSCARSSR_Python.cc:419-510)."""
+        params, paths = [], []
+        for pair in mapping or []:
+            if len(pair) != 2:
+                raise ValueError("Incorrect format in 'mapping'")
+            params.append(float(pair[0]))
+            f = pair[1]
+            paths.append(f if isinstance(f, bytes) else str(f).encode())
+        if not iformat:
+            raise ValueError("'iformat' is blank")
+        rot = _opt3(rotations, "rotations")
+        tr = _opt3(translation, "translation")
+        sc = [float(s) for s in (scale or [])]
+        parr = (C.c_double * max(1, len(params)))(*params)
+        farr = (C.c_char_p * max(1, len(paths)))(*paths)
+        scarr = (C.c_double * max(1, len(sc)))(*sc)
+        st = lib.srs_sim_add_bfield_interpolated(self._h, parr, farr, len(params), str(iformat).encode(),
+                                                 float(parameter), v3(rot), v3(tr), scarr, len(sc))
+        if st != _lib.SRS_OK:
+            raise ValueError("Could not import magnetic field.  Check filenames and 'iformat' are correct")
+
     def add_bfield_gaussian(self, bfield, sigma, rotations=None, translation=None):
         b = _list3(bfield, "bfield")
         s = _list3(sigma, "sigma")

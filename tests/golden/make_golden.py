@@ -394,9 +394,125 @@ def aggregate():
     save("aggregate.npz", **out)
 
 
+def field_file_cases(td):
+    """Synthetic field files in each of the reference's formats (seeded) and the add_bfield_* calls that
+    read them: (name, kind, arguments, evaluation points).  Written by make_golden.py into the
+    fixture, so the tests rebuild the same files without the generator."""
+    rng = np.random.default_rng(11)
+    cases = []
+    # OSCARS1D: irregular z samples, unsorted, a comment line, blank and '#' lines, three columns in the
+    # order Z By Bx with scale factors
+    z = np.sort(rng.uniform(-0.8, 0.8, 400))
+    z[0], z[-1] = -0.8, 0.8
+    rng.shuffle(z)
+    by = np.sin(2 * np.pi * z / 0.049) * 0.9
+    bx = 0.1 * np.cos(2 * np.pi * z / 0.07)
+    lines = ["# OSCARS1D test map"]
+    for k, (a, b, c) in enumerate(zip(z, by, bx)):
+        if k % 97 == 5:
+            lines.append("")
+        if k % 131 == 7:
+            lines.append("# a comment")
+        lines.append(f"{float(a)!r} {float(b)!r} {float(c)!r}")
+    p1 = os.path.join(td, "map1d.txt")
+    with open(p1, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    pts1 = np.column_stack([rng.uniform(-1e-3, 1e-3, 300), rng.uniform(-1e-3, 1e-3, 300), rng.uniform(-0.85, 0.85, 300)])
+    cases.append(("oscars1d", "file", dict(ifile=p1, iformat="OSCARS1D Z By Bx", scale=[1.0, 0.95, 1.2]), pts1))
+    cases.append(("oscars1d_rot", "file", dict(ifile=p1, iformat="oscars1d Z By Bx", rotations=[0.0, 0.01, 0.02],
+                                               translation=[0.0, 0.0, 0.05]), pts1))
+    # SRW: a 2-D (x, z) grid with '#' header values
+    nx, nz = 5, 161
+    xs, dx, zs, dz = -0.002, 0.001, -0.4, 0.005
+    lines = ["# SRW test map", f"#{xs!r}", f"#{dx!r}", f"#{nx}", "#0.0", "#0.0", "#1", f"#{zs!r}", f"#{dz!r}", f"#{nz}"]
+    for ix in range(nx):
+        for iz in range(nz):
+            zz = zs + iz * dz
+            lines.append(f"{0.01 * ix!r} {float(np.sin(zz * 40.0))!r} {float(0.001 * zz)!r}")
+    p2 = os.path.join(td, "srw.txt")
+    with open(p2, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    pts2 = np.column_stack([rng.uniform(-0.0025, 0.0025, 300), rng.uniform(-1e-3, 1e-3, 300), rng.uniform(-0.45, 0.45, 300)])
+    cases.append(("srw", "file", dict(ifile=p2, iformat="SRW"), pts2))
+    # SPECTRA: a 3-D grid, steps in mm, centred on 0
+    sx, sy, sz, mx, my, mz = 1.0, 2.0, 5.0, 3, 3, 81
+    lines = ["SPECTRA test map", f"{sx!r} {sy!r} {sz!r} {mx} {my} {mz}"]
+    for ix in range(mx):
+        for iy in range(my):
+            for iz in range(mz):
+                lines.append(f"{0.001 * (ix + iy)!r} {float(np.cos(iz * 0.3)) * (1 + 0.1 * ix)!r} {0.002 * iy!r}")
+    p3 = os.path.join(td, "spectra.txt")
+    with open(p3, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    pts3 = np.column_stack([rng.uniform(-0.0012, 0.0012, 300), rng.uniform(-0.0025, 0.0025, 300), rng.uniform(-0.22, 0.22, 300)])
+    cases.append(("spectra", "file", dict(ifile=p3, iformat="SPECTRA", rotations=[0.003, 0.0, 0.0]), pts3))
+    # interpolated OSCARS maps (gap scan): three files, mapping unsorted
+    paths = []
+    for gap, amp in ((15.0, 1.2), (25.0, 0.6), (20.0, 0.85)):
+        n = 201
+        lines = [f"# gap {gap}", "0", "0", "1", "0", "0", "1", "-0.5", "0.005", f"{n}"]
+        for iz in range(n):
+            zz = -0.5 + iz * 0.005
+            lines.append(f"0 {amp * float(np.sin(2 * np.pi * zz / 0.05))!r} {0.01 * amp!r}")
+        pth = os.path.join(td, f"gap{int(gap)}.txt")
+        with open(pth, "w") as fh:
+            fh.write("\n".join(lines) + "\n")
+        paths.append((gap, pth))
+    pts4 = np.column_stack([np.zeros(300), np.zeros(300), rng.uniform(-0.55, 0.55, 300)])
+    mapping = [[g, p] for g, p in paths]
+    cases.append(("interp", "interpolated", dict(mapping=mapping, iformat="OSCARS", parameter=18.3,
+                                                  scale=[1.0, 1.0, 1.1, 1.0, 0.9]), pts4))
+    cases.append(("interp_top", "interpolated", dict(mapping=mapping, iformat="OSCARS", parameter=25.0), pts4))
+    cases.append(("interp_first", "interpolated", dict(mapping=mapping, iformat="OSCARS", parameter=15.0), pts4))
+    return cases
+
+
+def field_files():
+    """add_bfield_file / add_bfield_interpolated on files of every format: the reference's field at
+    seeded points (src/TField3D_Grid.cc:25-45, 533-1446, OSCARSSR_Python.cc:337-510)."""
+    out, meta = {}, {}
+    with tempfile.TemporaryDirectory() as td:
+        for name, kind, kw, pts in field_file_cases(td):
+            o = new_sr()
+            args = dict(kw)
+            if kind == "file":
+                args["ifile"] = args["ifile"]
+                o.add_bfield_file(**args)
+                files = [args["ifile"]]
+            else:
+                args["mapping"] = [[g, p.encode()] for g, p in args["mapping"]]
+                o.add_bfield_interpolated(**args)
+                files = [p for _, p in kw["mapping"]]
+            out[f"{name}_points"] = pts
+            out[f"{name}_b"] = np.array([o.get_bfield(list(map(float, p))) for p in pts])
+            for k, fpath in enumerate(files):
+                out[f"{name}_file{k}"] = np.frombuffer(open(fpath, "rb").read(), dtype=np.uint8)
+            m = {kk: vv for kk, vv in kw.items() if kk not in ("ifile", "mapping")}
+            if kind == "interpolated":
+                m["mapping_params"] = [g for g, _ in kw["mapping"]]
+            meta[name] = dict(kind=kind, nfiles=len(files), **m)
+        # errors: lower-case column names, an unknown format, a parameter outside the mapping
+        errs = {}
+        o = new_sr()
+        p1 = os.path.join(td, "x.txt")
+        with open(p1, "w") as fh:
+            fh.write("# c\n0 1\n0.1 2\n")
+        for key, call in (("oscars1d_lowercase_columns", lambda: o.add_bfield_file(ifile=p1, iformat="OSCARS1D z by")),
+                          ("unknown_format", lambda: o.add_bfield_file(ifile=p1, iformat="FOO"))):
+            try:
+                call()
+                errs[key] = None
+            except ValueError as exc:
+                errs[key] = str(exc)
+        meta["errors"] = errs
+    with open(os.path.join(HERE, "field_files.json"), "w") as fh:
+        json.dump(meta, fh, indent=1)
+    save("field_files.npz", **out)
+
+
 if __name__ == "__main__":
     parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "beam32", "points", "grid", "adjoint",
-                             "quirks", "aggregate"]
+                             "quirks", "aggregate", "fieldfiles"]
     if "cfg0" in parts:
         e1 = cfg0()
         print("E1 (first-harmonic peak of the config-0 spectrum):", repr(e1))
@@ -407,6 +523,6 @@ if __name__ == "__main__":
     for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("beam32", beam32), ("points", points_surface),
                      ("grid", grid),
                      ("adjoint", adjoint),
-                     ("quirks", quirks), ("aggregate", aggregate)):
+                     ("quirks", quirks), ("aggregate", aggregate), ("fieldfiles", field_files)):
         if name in parts:
             fn()
