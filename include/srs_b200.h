@@ -51,6 +51,10 @@ int srs_device_count(void);
 /* ------------------------------------------------------------------ fields */
 
 enum { SRS_FIELD_UNDULATOR = 1, SRS_FIELD_GAUSSIAN = 2, SRS_FIELD_UNIFORM_BOX = 3, SRS_FIELD_GRID = 4 };
+/* kind | SRS_FIELD_ELECTRIC: an electric field [V/m] of the same shape, in the reference's separate
+ * electric-field container (OSCARSSR.cc:202-234).  With electric fields the RK4 derivative is
+ * q/(m gamma) E alone or q/(m gamma) (E + v x B) (DerivativesE / DerivativesEB, OSCARSSR.cc:690-793). */
+enum { SRS_FIELD_ELECTRIC = 0x100, SRS_FIELD_SHAPE_MASK = 0xff };
 
 /* One magnetic-field object in the form the reference keeps after construction:
  *  undulator (TField3D_IdealUndulator.cc): field and period already rotated, center, nperiods,
@@ -355,7 +359,29 @@ srs_status srs_read_field_interpolated(const double *parameters, const char *con
 srs_status srs_sim_add_bfield_grid(srs_sim *sim, const double start[3], const double step[3],
                                    const int64_t n[3], const double *data, const double rotations[3],
                                    const double translation[3]);
+/* Remove the magnetic fields (OSCARSSR::ClearMagneticFields); the electric fields stay. */
 srs_status srs_sim_clear_bfields(srs_sim *sim);
+/* Electric fields [V/m] (OSCARSSR_Python.cc:876-1390): the same shapes and arguments as the magnetic
+ * ones (the undulator without taper, the file without scaling); they enter the RK4 as
+ * q/(m gamma) E (DerivativesE / DerivativesEB, OSCARSSR.cc:690-793).  Trajectories with electric
+ * fields are always integrated serially. */
+srs_status srs_sim_add_efield_undulator(srs_sim *sim, const double efield[3], const double period[3],
+                                        int32_t nperiods, double phase, const double rotations[3],
+                                        const double translation[3]);
+srs_status srs_sim_add_efield_gaussian(srs_sim *sim, const double efield[3], const double sigma[3],
+                                       const double rotations[3], const double translation[3]);
+srs_status srs_sim_add_efield_uniform(srs_sim *sim, const double efield[3], const double width[3],
+                                      const double rotations[3], const double translation[3]);
+srs_status srs_sim_add_efield_file(srs_sim *sim, const char *path, const char *format,
+                                   const double rotations[3], const double translation[3]);
+srs_status srs_sim_clear_efields(srs_sim *sim);
+/* Electric field at points (device evaluation), HOST arrays of 3*np doubles. */
+srs_status srs_sim_get_efield(srs_sim *sim, const double *xyz, int64_t np, double *out);
+/* The time-domain electric field of the current particle at obs
+ * (OSCARSSR::CalculateElectricFieldTimeDomain, OSCARSSR.cc:2646-2690): for every trajectory point, in
+ * time order, the arrival time t [s] (HOST, *n doubles) and the field [V/m] (HOST, 3 * *n doubles).
+ * With t or e NULL, *n returns the number of points. */
+srs_status srs_sim_calculate_efield_time(srs_sim *sim, const double obs[3], double *t, double *e, int64_t *n);
 /* The object keeps the device trajectory of its last single-particle calculation and reuses it
  * while the particle, the fields and the trajectory settings are unchanged (the reference recomputes
  * the identical trajectory on every call).  enabled = 0 turns this off; every call drops the kept

@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libsrs_b200.so")
 
 SRS_OK, SRS_ERR_INVALID, SRS_ERR_RANGE, SRS_ERR_CUDA, SRS_ERR_NO_DEVICE, SRS_ERR_TIMEOUT, SRS_ERR_IO = range(7)
 UNDULATOR, GAUSSIAN, UNIFORM_BOX, GRID = 1, 2, 3, 4
+ELECTRIC = 0x100  # kind flag of an electric field
 FP64, MIXED = 0, 1
 
 _D = C.POINTER(C.c_double)
@@ -109,6 +110,13 @@ def _load():
                                             _D, C.c_int32, C.POINTER(Field), _D, C.POINTER(C.c_int64)]),
         "srs_sim_add_bfield_grid": (S, [P, _D, _D, C.POINTER(C.c_int64), _D, _D, _D]),
         "srs_sim_clear_bfields": (S, [P]),
+        "srs_sim_clear_efields": (S, [P]),
+        "srs_sim_add_efield_undulator": (S, [P, _D, _D, C.c_int32, C.c_double, _D, _D]),
+        "srs_sim_add_efield_gaussian": (S, [P, _D, _D, _D, _D]),
+        "srs_sim_add_efield_uniform": (S, [P, _D, _D, _D, _D]),
+        "srs_sim_add_efield_file": (S, [P, C.c_char_p, C.c_char_p, _D, _D]),
+        "srs_sim_get_efield": (S, [P, _D, C.c_int64, _D]),
+        "srs_sim_calculate_efield_time": (S, [P, _D, _D, _D, C.POINTER(C.c_int64)]),
         "srs_sim_set_trajectory_cache": (S, [P, C.c_int32]),
         "srs_sim_set_trajectory_mode": (S, [P, C.c_int32]),
         "srs_sim_get_nfields": (C.c_int32, [P]),
@@ -166,7 +174,7 @@ EXPORTED = (
     "srs_sim_set_ctstartstop srs_sim_set_npoints_trajectory srs_sim_get_ctstartstop "
     "srs_sim_get_npoints_trajectory srs_sim_set_nthreads_global srs_sim_set_gpu_global "
     "srs_sim_add_bfield_undulator srs_sim_add_bfield_gaussian srs_sim_add_bfield_uniform "
-    "srs_read_field_file srs_read_field_interpolated srs_sim_add_bfield_interpolated srs_sim_add_bfield_file srs_sim_add_bfield_grid srs_sim_clear_bfields srs_sim_get_nfields "
+    "srs_read_field_file srs_read_field_interpolated srs_sim_add_bfield_interpolated srs_sim_add_bfield_file srs_sim_add_bfield_grid srs_sim_clear_efields srs_sim_add_efield_undulator srs_sim_add_efield_gaussian srs_sim_add_efield_uniform srs_sim_add_efield_file srs_sim_get_efield srs_sim_calculate_efield_time srs_sim_clear_bfields srs_sim_get_nfields "
     "srs_sim_set_trajectory_cache srs_sim_set_trajectory_mode "
     "srs_sim_get_bfield srs_sim_set_field_grid_data srs_sim_add_particle_beam "
     "srs_sim_clear_particle_beams srs_sim_get_nparticle_beams srs_sim_set_new_particle "

@@ -643,6 +643,7 @@ srs_status srs_trajectory_adjoint(const srs_field *fields, int32_t nfields, cons
   if (!particle || !d_x || !d_beta || !d_gx || !d_gbeta || !ic_grad) return fail(SRS_ERR_INVALID, "NULL argument");
   if (nfields < 0 || nfields > kAdjMaxFields || (nfields > 0 && !fields))
     return fail(SRS_ERR_INVALID, "the adjoint takes 0.." + std::to_string(kAdjMaxFields) + " fields");
+  if (has_electric(fields, nfields)) return fail(SRS_ERR_INVALID, "the adjoint takes magnetic fields only");
   double dt;
   int64_t nf, nb;
   if (srs_status st = srs_trajectory_counts(ctstart, ctstop, t0, npoints, &dt, &nf, &nb)) return st;

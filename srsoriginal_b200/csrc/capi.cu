@@ -80,7 +80,7 @@ srs_status srs_trajectory(const srs_field *fields, int32_t nfields, const srs_pa
   if (nparticles < 1 || !particles) return fail(SRS_ERR_INVALID, "bad particle array");
   if (!d_x || !d_beta || !d_aoc) return fail(SRS_ERR_INVALID, "output pointers are NULL");
   for (int i = 0; i < nfields; ++i)
-    if (fields[i].kind == SRS_FIELD_GRID && !fields[i].data)
+    if (field_shape(fields[i].kind) == SRS_FIELD_GRID && !fields[i].data)
       return fail(SRS_ERR_INVALID, "grid field without data");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   DeviceBuffer df, dp;
@@ -89,7 +89,7 @@ srs_status srs_trajectory(const srs_field *fields, int32_t nfields, const srs_pa
   if (nfields > 0) SRS_CUDA(cudaMemcpyAsync(df.ptr, fields, sizeof(srs_field) * nfields, cudaMemcpyHostToDevice, s));
   SRS_CUDA(cudaMemcpyAsync(dp.ptr, particles, sizeof(srs_particle) * nparticles, cudaMemcpyHostToDevice, s));
   SRS_CUDA(launch_rk4(df.as<srs_field>(), nfields, dp.as<srs_particle>(), nparticles, dt, nf, nb, d_x, d_beta, d_aoc, s,
-                      nfields > 0 ? grid_stage_doubles(fields, nfields) : 0));
+                      nfields > 0 ? grid_stage_doubles(fields, nfields) : 0, has_electric(fields, nfields)));
   return SRS_OK;
 }
 
@@ -108,7 +108,7 @@ srs_status srs_trajectory_shoot(const srs_field *fields, int32_t nfields, const 
   if (steps_per_segment < 0) return fail(SRS_ERR_INVALID, "steps_per_segment must be >= 0");
   if (max_iterations < 0 || max_iterations > 32) return fail(SRS_ERR_INVALID, "max_iterations must be in [0, 32]");
   for (int i = 0; i < nfields; ++i)
-    if (fields[i].kind == SRS_FIELD_GRID && !fields[i].data)
+    if (field_shape(fields[i].kind) == SRS_FIELD_GRID && !fields[i].data)
       return fail(SRS_ERR_INVALID, "grid field without data");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   DeviceBuffer df, dp, scratch;
@@ -117,6 +117,12 @@ srs_status srs_trajectory_shoot(const srs_field *fields, int32_t nfields, const 
   SRS_CUDA(scratch.alloc(shoot_scratch_bytes(nf, nb, steps_per_segment, nfields), s));
   if (nfields > 0) SRS_CUDA(cudaMemcpyAsync(df.ptr, fields, sizeof(srs_field) * nfields, cudaMemcpyHostToDevice, s));
   SRS_CUDA(cudaMemcpyAsync(dp.ptr, particle, sizeof(srs_particle), cudaMemcpyHostToDevice, s));
+  if (has_electric(fields, nfields)) {  // electric fields: the serial kernel (its statistics say 0 iterations)
+    SRS_CUDA(launch_rk4(df.as<srs_field>(), nfields, dp.as<srs_particle>(), 1, dt, nf, nb, d_x, d_beta, d_aoc, s,
+                        grid_stage_doubles(fields, nfields), true));
+    if (d_stats) SRS_CUDA(cudaMemsetAsync(d_stats, 0, sizeof(double) * 4, s));
+    return SRS_OK;
+  }
   SRS_CUDA(launch_rk4_shoot(df.as<srs_field>(), nfields, dp.as<srs_particle>(), *particle, dt, nf, nb, d_x, d_beta,
                             d_aoc, s, nfields > 0 ? grid_stage_doubles(fields, nfields) : 0, steps_per_segment,
                             max_iterations, scratch.ptr, d_stats));

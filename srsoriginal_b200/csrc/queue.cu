@@ -307,7 +307,7 @@ srs_status srs_trajectory_batch(const srs_field *fields, int32_t nfields, const 
   SRS_CUDA(cudaMemcpyAsync(dp.ptr, particles, sizeof(srs_particle) * nparticles, cudaMemcpyHostToDevice, s));
   SRS_CUDA(cudaMemcpyAsync(ds.ptr, specs.data(), sizeof(TrajSpec) * nparticles, cudaMemcpyHostToDevice, s));
   SRS_CUDA(launch_rk4_specs(df.as<srs_field>(), nfields, dp.as<srs_particle>(), ds.as<TrajSpec>(), nparticles, s,
-                            nfields > 0 ? grid_stage_doubles(fields, nfields) : 0));
+                            nfields > 0 ? grid_stage_doubles(fields, nfields) : 0, has_electric(fields, nfields)));
   return SRS_OK;
 }
 

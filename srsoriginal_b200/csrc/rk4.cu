@@ -40,7 +40,7 @@ namespace {
 // With specs != nullptr each particle has its own time step, point counts and output arrays (jobs of
 // different trajectory lengths); a warp then runs its longest particle's step count, and groups whose
 // trajectory is complete keep stepping without storing.
-template <int G>
+template <int G, bool kE>
 __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restrict__ gfields, int nfields,
                                                        const srs_particle *__restrict__ particles, int nparticles,
                                                        double dt_all, int64_t nfwd_all, int64_t nbwd_all,
@@ -96,17 +96,36 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   }
   const Prepared &fp = G == 32 ? myp : sp[fidx];
   const srs_field &ff = G == 32 ? myf : sf[fidx];
-  // B at two positions, one per slot, summed over fields in field order
-  auto fields2 = [&](V3 pa, V3 pb, V3 &Ba, V3 &Bb) {
+  // B (and with kE, E) at two positions, one per slot, each summed over its fields in field order
+  bool has_b = true;  // kE: whether the magnetic container has fields (DerivativesE / DerivativesEB)
+  if (kE) {
+    has_b = false;
+    for (int f = 0; f < nfields; ++f) has_b = has_b || !field_electric(sf[f].kind);
+  }
+  auto fields2 = [&](V3 pa, V3 pb, V3 &Ba, V3 &Bb, V3 &Ea, V3 &Eb) {
     V3 mine = v3(0, 0, 0);
     if (nfields > 0) mine = field_one(fp, ff, slot == 0 ? pa : pb);
     Ba = v3(0, 0, 0);
     Bb = v3(0, 0, 0);
+    Ea = v3(0, 0, 0);
+    Eb = v3(0, 0, 0);
     for (int f = 0; f < nfields; ++f) {
       const int la = gbase + f, lb = gbase + nfields + f;
-      Ba = Ba + v3(__shfl_sync(full, mine.x, la), __shfl_sync(full, mine.y, la), __shfl_sync(full, mine.z, la));
-      Bb = Bb + v3(__shfl_sync(full, mine.x, lb), __shfl_sync(full, mine.y, lb), __shfl_sync(full, mine.z, lb));
+      const V3 va = v3(__shfl_sync(full, mine.x, la), __shfl_sync(full, mine.y, la), __shfl_sync(full, mine.z, la));
+      const V3 vb = v3(__shfl_sync(full, mine.x, lb), __shfl_sync(full, mine.y, lb), __shfl_sync(full, mine.z, lb));
+      if (kE && field_electric(sf[f].kind)) {
+        Ea = Ea + va;
+        Eb = Eb + vb;
+      } else {
+        Ba = Ba + va;
+        Bb = Bb + vb;
+      }
     }
+  };
+  // the velocity part of the derivative: DerivativesB, or with kE DerivativesE / DerivativesEB
+  auto accel = [&](V3 v, V3 Bv, V3 Ev) -> V3 {
+    if (!kE) return force(qomg, v, Bv);
+    return has_b ? force_eb(qomg, v, Ev, Bv) : force_e(qomg, Ev);
   };
   // the group's lanes store the nine components of a point (x, y, z, beta = v/c, a/c), lane gl taking
   // components gl, gl + G, ...; selects, not branches
@@ -127,21 +146,21 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
   // one RK4 step of size h from (pos, vel); returns the derivative at the start state (its velocity part)
   auto step = [&](V3 &pos, V3 &vel, double h) -> V3 {
     const double hh = h * 0.5, h6 = h / 6.0;
-    V3 B1, B2, B3, B4;
+    V3 B1, B2, B3, B4, E1, E2, E3, E4;
     const V3 p2 = vadd_scaled(pos, hh, vel);          // yt = y + hh*dydx (positions)
-    fields2(pos, p2, B1, B2);
-    const V3 a1 = force(qomg, vel, B1);                // dydx (velocity part)
+    fields2(pos, p2, B1, B2, E1, E2);
+    const V3 a1 = accel(vel, B1, E1);                  // dydx (velocity part)
     const V3 v2 = vadd_scaled(vel, hh, a1);
-    const V3 a2 = force(qomg, v2, B2);                 // dyt
+    const V3 a2 = accel(v2, B2, E2);                   // dyt
     const V3 p3 = vadd_scaled(pos, hh, v2);            // yt = y + hh*dyt
     const V3 v3_ = vadd_scaled(vel, hh, a2);
     const V3 p4 = vadd_scaled(pos, h, v3_);            // yt = y + h*dym (positions need dym = dyt(p3) pos part = v3)
     // dym = f(yt3): position part v3_, velocity part a3 = force(v3_, B(p3))
-    fields2(p3, p4, B3, B4);
-    const V3 a3 = force(qomg, v3_, B3);
+    fields2(p3, p4, B3, B4, E3, E4);
+    const V3 a3 = accel(v3_, B3, E3);
     const V3 v4 = vadd_scaled(vel, h, a3);             // yt = y + h*dym (velocities)
     const V3 m_pos = v3_ + v2, m_vel = a3 + a2;        // dym += dyt
-    const V3 a4 = force(qomg, v4, B4);                 // dyt = f(yt4): position part v4
+    const V3 a4 = accel(v4, B4, E4);                   // dyt = f(yt4): position part v4
     // yout = y + h6*(dydx + dyt + 2.0*dym)
     const V3 npos = v3(pos.x + h6 * (vel.x + v4.x + 2.0 * m_pos.x), pos.y + h6 * (vel.y + v4.y + 2.0 * m_pos.y),
                        pos.z + h6 * (vel.z + v4.z + 2.0 * m_pos.z));
@@ -170,6 +189,7 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
 
 // ---------------------------------------------------------------- one thread per particle
 
+template <bool kE>
 __global__ void __launch_bounds__(64) rk4_thread_kernel(const srs_field *__restrict__ gfields, int nfields,
                                                         const srs_particle *__restrict__ particles, int nparticles,
                                                         double dt, int64_t nfwd, int64_t nbwd,
@@ -189,24 +209,35 @@ __global__ void __launch_bounds__(64) rk4_thread_kernel(const srs_field *__restr
   const int64_t n = nfwd + nbwd;
   double *xp = X + (int64_t)p * 3 * n, *bp = Bt + (int64_t)p * 3 * n, *ap = A + (int64_t)p * 3 * n;
   const double C = kC, qomg = P.qomg;
-  auto Bsum = [&](V3 x) {
+  // the magnetic (electric = false) or electric container's sum at x
+  auto Fsum = [&](V3 x, bool electric) {
     V3 s = v3(0, 0, 0);
-    for (int f = 0; f < nfields; ++f) s = s + field_one(sp[f], sf[f], x);
+    for (int f = 0; f < nfields; ++f)
+      if (!kE || field_electric(sf[f].kind) == electric) s = s + field_one(sp[f], sf[f], x);
     return s;
+  };
+  bool has_b = true;
+  if (kE) {
+    has_b = false;
+    for (int f = 0; f < nfields; ++f) has_b = has_b || !field_electric(sf[f].kind);
+  }
+  auto accel = [&](V3 v, V3 x) -> V3 {
+    if (!kE) return force(qomg, v, Fsum(x, false));
+    return has_b ? force_eb(qomg, v, Fsum(x, true), Fsum(x, false)) : force_e(qomg, Fsum(x, true));
   };
   auto step = [&](V3 &pos, V3 &vel, double h) -> V3 {
     const double hh = h * 0.5, h6 = h / 6.0;
     const V3 p2 = vadd_scaled(pos, hh, vel);
-    const V3 a1 = force(qomg, vel, Bsum(pos));
+    const V3 a1 = accel(vel, pos);
     const V3 v2 = vadd_scaled(vel, hh, a1);
-    const V3 a2 = force(qomg, v2, Bsum(p2));
+    const V3 a2 = accel(v2, p2);
     const V3 p3 = vadd_scaled(pos, hh, v2);
     const V3 v3_ = vadd_scaled(vel, hh, a2);
-    const V3 a3 = force(qomg, v3_, Bsum(p3));
+    const V3 a3 = accel(v3_, p3);
     const V3 p4 = vadd_scaled(pos, h, v3_);
     const V3 v4 = vadd_scaled(vel, h, a3);
     const V3 m_pos = v3_ + v2, m_vel = a3 + a2;
-    const V3 a4 = force(qomg, v4, Bsum(p4));
+    const V3 a4 = accel(v4, p4);
     const V3 npos = v3(pos.x + h6 * (vel.x + v4.x + 2.0 * m_pos.x), pos.y + h6 * (vel.y + v4.y + 2.0 * m_pos.y),
                        pos.z + h6 * (vel.z + v4.z + 2.0 * m_pos.z));
     const V3 nvel = v3(vel.x + h6 * (a1.x + a4.x + 2.0 * m_vel.x), vel.y + h6 * (a1.y + a4.y + 2.0 * m_vel.y),
@@ -237,10 +268,10 @@ __global__ void __launch_bounds__(64) rk4_thread_kernel(const srs_field *__restr
 }
 
 __global__ void field_eval_kernel(const srs_field *__restrict__ fields, int nfields, const double *__restrict__ xyz,
-                                  int64_t np, double *__restrict__ out) {
+                                  int64_t np, double *__restrict__ out, int electric) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= np) return;
-  V3 b = field_sum(fields, nfields, v3(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+  V3 b = field_sum(fields, nfields, v3(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]), electric != 0);
   out[3 * i] = b.x;
   out[3 * i + 1] = b.y;
   out[3 * i + 2] = b.z;
@@ -265,7 +296,7 @@ static int group_size(int nparticles, int nfields) {
 int64_t grid_stage_doubles(const srs_field *host_fields, int nfields) {
   int64_t total = 0;
   for (int i = 0; i < nfields; ++i)
-    if (host_fields[i].kind == SRS_FIELD_GRID)
+    if (field_shape(host_fields[i].kind) == SRS_FIELD_GRID)
       total += 3 * host_fields[i].n[0] * host_fields[i].n[1] * host_fields[i].n[2];
   return total <= kGridStageMaxDoubles ? total : 0;
 }
@@ -280,41 +311,58 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 }
 }  // namespace
 
-template <int G>
+template <int G, bool kE>
 static cudaError_t launch_warp_rk4_g(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
                               double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
                               const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s,
                               const int *d_skip = nullptr) {
   const size_t smem = sizeof(double) * (size_t)stage_doubles;
-  if (cudaError_t e = allow_smem(rk4_warp_kernel<G>, smem)) return e;
+  if (cudaError_t e = allow_smem(rk4_warp_kernel<G, kE>, smem)) return e;
   const int warps = 4, per_block = G == 32 ? 1 : warps * (32 / G);
-  rk4_warp_kernel<G><<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
+  rk4_warp_kernel<G, kE><<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
       d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, d_specs, stage_doubles, d_skip);
   return cudaGetLastError();
 }
 
-static cudaError_t launch_warp_rk4(int G, const srs_field *d_fields, int nfields, const srs_particle *d_particles,
-                            int nparticles, double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b,
-                            double *d_a, const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s,
-                            const int *d_skip = nullptr) {
+template <bool kE>
+static cudaError_t launch_warp_rk4_e(int G, const srs_field *d_fields, int nfields, const srs_particle *d_particles,
+                                     int nparticles, double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b,
+                                     double *d_a, const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s,
+                                     const int *d_skip) {
   switch (G) {
-    case 2: return launch_warp_rk4_g<2>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+    case 2: return launch_warp_rk4_g<2, kE>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
                                         d_specs, stage_doubles, s, d_skip);
-    case 4: return launch_warp_rk4_g<4>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+    case 4: return launch_warp_rk4_g<4, kE>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
                                         d_specs, stage_doubles, s, d_skip);
-    case 8: return launch_warp_rk4_g<8>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+    case 8: return launch_warp_rk4_g<8, kE>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
                                         d_specs, stage_doubles, s, d_skip);
-    case 16: return launch_warp_rk4_g<16>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+    case 16: return launch_warp_rk4_g<16, kE>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
                                           d_specs, stage_doubles, s, d_skip);
-    case 32: return launch_warp_rk4_g<32>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
+    case 32: return launch_warp_rk4_g<32, kE>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
                                           d_specs, stage_doubles, s, d_skip);
     default: return cudaErrorInvalidValue;
   }
 }
 
+static cudaError_t launch_warp_rk4(int G, const srs_field *d_fields, int nfields, const srs_particle *d_particles,
+                                   int nparticles, double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b,
+                                   double *d_a, const TrajSpec *d_specs, int64_t stage_doubles, cudaStream_t s,
+                                   const int *d_skip = nullptr, bool electric = false) {
+  return electric ? launch_warp_rk4_e<true>(G, d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b,
+                                            d_a, d_specs, stage_doubles, s, d_skip)
+                  : launch_warp_rk4_e<false>(G, d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b,
+                                             d_a, d_specs, stage_doubles, s, d_skip);
+}
+
+bool has_electric(const srs_field *host_fields, int nfields) {
+  for (int i = 0; i < nfields; ++i)
+    if (field_electric(host_fields[i].kind)) return true;
+  return false;
+}
+
 cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
                        double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
-                       cudaStream_t s, int64_t stage_doubles) {
+                       cudaStream_t s, int64_t stage_doubles, bool electric) {
   if (nparticles <= 0) return cudaSuccess;
   if (nfields > kMaxFieldsShared) return cudaErrorInvalidValue;
   const size_t smem = sizeof(double) * (size_t)stage_doubles;
@@ -323,13 +371,19 @@ cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particl
   // per particle when there are enough particles to fill the SMs (issue rate is the limit)
   if (G <= 32 && (int64_t)nparticles * G <= 148 * 32 * 48) {
     if (cudaError_t e = launch_warp_rk4(G, d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a,
-                                        nullptr, stage_doubles, s))
+                                        nullptr, stage_doubles, s, nullptr, electric))
       return e;
   } else {
     const int threads = 64;
-    if (cudaError_t e = allow_smem(rk4_thread_kernel, smem)) return e;
-    rk4_thread_kernel<<<(nparticles + threads - 1) / threads, threads, smem, s>>>(
-        d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, stage_doubles);
+    if (electric) {
+      if (cudaError_t e = allow_smem(rk4_thread_kernel<true>, smem)) return e;
+      rk4_thread_kernel<true><<<(nparticles + threads - 1) / threads, threads, smem, s>>>(
+          d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, stage_doubles);
+    } else {
+      if (cudaError_t e = allow_smem(rk4_thread_kernel<false>, smem)) return e;
+      rk4_thread_kernel<false><<<(nparticles + threads - 1) / threads, threads, smem, s>>>(
+          d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, stage_doubles);
+    }
   }
   return cudaGetLastError();
 }
@@ -343,22 +397,24 @@ cudaError_t launch_rk4_unless(const srs_field *d_fields, int nfields, const srs_
 }
 
 cudaError_t launch_rk4_specs(const srs_field *d_fields, int nfields, const srs_particle *d_particles,
-                             const TrajSpec *d_specs, int nparticles, cudaStream_t s, int64_t stage_doubles) {
+                             const TrajSpec *d_specs, int nparticles, cudaStream_t s, int64_t stage_doubles,
+                             bool electric) {
   if (nparticles <= 0) return cudaSuccess;
   if (nfields > kMaxFieldsShared) return cudaErrorInvalidValue;
   const int G = group_size(nparticles, nfields);
   if (G > 32) return cudaErrorInvalidValue;
   if (cudaError_t e = launch_warp_rk4(G, d_fields, nfields, d_particles, nparticles, 0.0, 0, 0, nullptr, nullptr,
-                                      nullptr, d_specs, stage_doubles, s))
+                                      nullptr, d_specs, stage_doubles, s, nullptr, electric))
     return e;
   return cudaGetLastError();
 }
 
 cudaError_t launch_field_eval(const srs_field *d_fields, int nfields, const double *d_xyz, int64_t np,
-                              double *d_out, cudaStream_t s) {
+                              double *d_out, cudaStream_t s, bool electric) {
   if (np <= 0) return cudaSuccess;
   const int threads = 128;
-  field_eval_kernel<<<(unsigned)((np + threads - 1) / threads), threads, 0, s>>>(d_fields, nfields, d_xyz, np, d_out);
+  field_eval_kernel<<<(unsigned)((np + threads - 1) / threads), threads, 0, s>>>(d_fields, nfields, d_xyz, np, d_out,
+                                                                                 electric ? 1 : 0);
   return cudaGetLastError();
 }
 

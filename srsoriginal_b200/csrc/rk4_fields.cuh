@@ -26,7 +26,7 @@ struct Prepared {
 };
 
 __device__ void prepare(const srs_field &f, Prepared &p) {
-  p.kind = f.kind;
+  p.kind = field_shape(f.kind);
   p.gd = f.data;
   for (int c = 0; c < 3; ++c) p.rstep[c] = f.step[c] != 0 ? 1.0 / f.step[c] : 0.0;
   for (int c = 0; c < 3; ++c) {
@@ -35,7 +35,7 @@ __device__ void prepare(const srs_field &f, Prepared &p) {
     p.rs[c] = sin(f.rotations[c]);
     p.rc[c] = cos(f.rotations[c]);
   }
-  if (f.kind == SRS_FIELD_UNDULATOR) {
+  if (p.kind == SRS_FIELD_UNDULATOR) {
     // TField3D_IdealUndulator::Init (:62-80) and the per-call expressions of GetF (:106-139)
     const V3 per = ld3(f.period);
     p.plen = mag(per);
@@ -107,6 +107,14 @@ __device__ inline V3 force(double qomg, V3 v, V3 B) {
   return v3(qomg * (-v.z * B.y + v.y * B.z), qomg * (v.z * B.x - v.x * B.z), qomg * (v.x * B.y - v.y * B.x));
 }
 
+// DerivativesE and DerivativesEB (OSCARSSR.cc:713-793): q/(m gamma) E, and q/(m gamma) (E + v x B) in the
+// reference's operation order
+__device__ inline V3 force_e(double qomg, V3 E) { return v3(qomg * E.x, qomg * E.y, qomg * E.z); }
+__device__ inline V3 force_eb(double qomg, V3 v, V3 E, V3 B) {
+  return v3(qomg * (E.x - v.z * B.y + v.y * B.z), qomg * (E.y + v.z * B.x - v.x * B.z),
+            qomg * (E.z + v.x * B.y - v.y * B.x));
+}
+
 __device__ inline V3 vadd_scaled(V3 a, double h, V3 b) { return v3(a.x + h * b.x, a.y + h * b.y, a.z + h * b.z); }
 
 // Copies every grid field's samples into the block's dynamic shared memory (the launcher sizes it to
@@ -116,7 +124,7 @@ extern __shared__ __align__(16) double g_stage[];
 __device__ void stage_grids(const srs_field *sf, Prepared *sp, int nfields) {
   int64_t off = 0;
   for (int i = 0; i < nfields; ++i) {
-    if (sf[i].kind != SRS_FIELD_GRID) continue;
+    if (field_shape(sf[i].kind) != SRS_FIELD_GRID) continue;
     const int64_t cnt = 3 * sf[i].n[0] * sf[i].n[1] * sf[i].n[2];
     for (int64_t k = threadIdx.x; k < cnt; k += blockDim.x) g_stage[off + k] = sf[i].data[k];
     off += cnt;
@@ -125,7 +133,7 @@ __device__ void stage_grids(const srs_field *sf, Prepared *sp, int nfields) {
   if (threadIdx.x == 0) {
     off = 0;
     for (int i = 0; i < nfields; ++i) {
-      if (sf[i].kind != SRS_FIELD_GRID) continue;
+      if (field_shape(sf[i].kind) != SRS_FIELD_GRID) continue;
       sp[i].gd = g_stage + off;
       off += 3 * sf[i].n[0] * sf[i].n[1] * sf[i].n[2];
     }

@@ -200,10 +200,46 @@ struct srs_sim {
     return SRS_OK;
   }
 
+  // Removes the magnetic (electric = false) or the electric fields, keeping the others in order.
+  void remove_fields(bool electric) {
+    size_t k = 0;
+    for (size_t i = 0; i < fields.size(); ++i) {
+      if (field_electric(fields[i].kind) == electric) {
+        if (grid_dev[i]) cudaFree(grid_dev[i]);
+        continue;
+      }
+      fields[k] = fields[i];
+      grid_host[k] = std::move(grid_host[i]);
+      grid_dev[k] = grid_dev[i];
+      ++k;
+    }
+    fields.resize(k);
+    grid_host.resize(k);
+    grid_dev.resize(k);
+    fields_dirty = true;
+    ++fields_version;
+  }
+
+  // The magnetic or electric field at np points (HOST arrays of 3 np doubles), evaluated on the device.
+  srs_status eval_fields(const double *xyz, int64_t np, double *out, bool electric) {
+    if (!xyz || !out || np < 0) return fail(SRS_ERR_INVALID, "bad argument");
+    if (np == 0) return SRS_OK;
+    if (srs_status st = upload_fields()) return st;
+    DeviceBuffer dx, dout;
+    SRS_CUDA(dx.alloc(sizeof(double) * 3 * np, stream));
+    SRS_CUDA(dout.alloc(sizeof(double) * 3 * np, stream));
+    SRS_CUDA(cudaMemcpyAsync(dx.ptr, xyz, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, stream));
+    SRS_CUDA(launch_field_eval(reinterpret_cast<const srs_field *>(d_fields), (int)fields.size(), dx.as<double>(), np,
+                               dout.as<double>(), stream, electric));
+    SRS_CUDA(cudaMemcpyAsync(out, dout.ptr, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost, stream));
+    SRS_CUDA(cudaStreamSynchronize(stream));
+    return SRS_OK;
+  }
+
   srs_status add_field(const srs_field &f, std::vector<double> &&host_grid) {
     double *dev = nullptr;
     srs_field g = f;
-    if (f.kind == SRS_FIELD_GRID) {
+    if (field_shape(f.kind) == SRS_FIELD_GRID) {
       SRS_CUDA(cudaMalloc(&dev, sizeof(double) * host_grid.size()));
       SRS_CUDA(cudaMemcpy(dev, host_grid.data(), sizeof(double) * host_grid.size(), cudaMemcpyHostToDevice));
       g.data = dev;
@@ -301,7 +337,8 @@ struct srs_sim {
     SRS_CUDA(dp.alloc(sizeof(srs_particle) * np, stream));
     SRS_CUDA(cudaMemcpyAsync(dp.ptr, hp.data(), sizeof(srs_particle) * np, cudaMemcpyHostToDevice, stream));
     const int64_t stage = fields.empty() ? 0 : grid_stage_doubles(fields.data(), (int)fields.size());
-    if (shoot && np == 1 && n >= kShootMinPoints) {
+    const bool electric = has_electric(fields.data(), (int)fields.size());
+    if (shoot && !electric && np == 1 && n >= kShootMinPoints) {
       DeviceBuffer scratch;
       SRS_CUDA(scratch.alloc(shoot_scratch_bytes(nf, nb, 0, (int)fields.size()), stream));
       SRS_CUDA(launch_rk4_shoot(reinterpret_cast<const srs_field *>(d_fields), (int)fields.size(),
@@ -309,7 +346,7 @@ struct srs_sim {
                                 nullptr));
     } else {
       SRS_CUDA(launch_rk4(reinterpret_cast<const srs_field *>(d_fields), (int)fields.size(), dp.as<srs_particle>(), np,
-                          dt, nf, nb, X, B, A, stream, stage));
+                          dt, nf, nb, X, B, A, stream, stage, electric));
     }
     view.x = X;
     view.beta = B;
@@ -641,13 +678,99 @@ srs_status srs_sim_add_bfield_grid(srs_sim *sim, const double start[3], const do
 
 srs_status srs_sim_clear_bfields(srs_sim *sim) {
   SIM_GUARD(sim);
-  for (double *p : sim->grid_dev)
-    if (p) cudaFree(p);
-  sim->fields.clear();
-  sim->grid_host.clear();
-  sim->grid_dev.clear();
-  sim->fields_dirty = true;
-  ++sim->fields_version;
+  sim->remove_fields(false);
+  return SRS_OK;
+}
+
+srs_status srs_sim_clear_efields(srs_sim *sim) {
+  SIM_GUARD(sim);
+  sim->remove_fields(true);
+  return SRS_OK;
+}
+
+// ---------------------------------------------------------------- electric fields
+// The reference's electric-field container (OSCARSSR.cc:202-234, OSCARSSR_Python.cc:876-1390): the same
+// shapes as the magnetic ones, marked SRS_FIELD_ELECTRIC.
+
+srs_status srs_sim_add_efield_undulator(srs_sim *sim, const double efield[3], const double period[3], int32_t nperiods,
+                                        double phase, const double rotations[3], const double translation[3]) {
+  SIM_GUARD(sim);
+  srs_field f;
+  std::memset(&f, 0, sizeof f);
+  f.kind = SRS_FIELD_UNDULATOR | SRS_FIELD_ELECTRIC;  // OSCARSSR_Python.cc:1156-1240 (no taper)
+  put(f.field, rot(vec(efield), rotations));
+  put(f.period, rot(vec(period), rotations));
+  std::memcpy(f.center, translation, sizeof(double) * 3);
+  f.nperiods = nperiods;
+  f.phase = phase;
+  return sim->add_field(f, {});
+}
+
+srs_status srs_sim_add_efield_gaussian(srs_sim *sim, const double efield[3], const double sigma[3],
+                                       const double rotations[3], const double translation[3]) {
+  SIM_GUARD(sim);
+  srs_field f;
+  std::memset(&f, 0, sizeof f);
+  f.kind = SRS_FIELD_GAUSSIAN | SRS_FIELD_ELECTRIC;
+  put(f.field, rot(vec(efield), rotations));
+  std::memcpy(f.center, translation, sizeof(double) * 3);
+  std::memcpy(f.sigma_or_width, sigma, sizeof(double) * 3);
+  std::memcpy(f.rotations, rotations, sizeof(double) * 3);
+  return sim->add_field(f, {});
+}
+
+srs_status srs_sim_add_efield_uniform(srs_sim *sim, const double efield[3], const double width[3],
+                                      const double rotations[3], const double translation[3]) {
+  SIM_GUARD(sim);
+  srs_field f;
+  std::memset(&f, 0, sizeof f);
+  f.kind = SRS_FIELD_UNIFORM_BOX | SRS_FIELD_ELECTRIC;
+  put(f.field, rot(vec(efield), rotations));
+  std::memcpy(f.center, translation, sizeof(double) * 3);
+  std::memcpy(f.sigma_or_width, width, sizeof(double) * 3);
+  std::memcpy(f.rotations, rotations, sizeof(double) * 3);
+  return sim->add_field(f, {});
+}
+
+srs_status srs_sim_add_efield_file(srs_sim *sim, const char *path, const char *format, const double rotations[3],
+                                   const double translation[3]) {
+  SIM_GUARD(sim);
+  if (!path || !format || !*path || !*format) return fail(SRS_ERR_INVALID, "'ifile' or 'iformat' is blank");
+  srs_field f;
+  std::vector<double> data;
+  // OSCARSSR::AddElectricField (OSCARSSR.cc:202-211): the grid reader without scaling
+  if (srs_status st = read_field_file(path, format, rotations, translation, nullptr, 0, f, data)) return st;
+  f.kind |= SRS_FIELD_ELECTRIC;
+  return sim->add_field(f, std::move(data));
+}
+
+srs_status srs_sim_get_efield(srs_sim *sim, const double *xyz, int64_t np, double *out) {
+  SIM_GUARD(sim);
+  return sim->eval_fields(xyz, np, out, true);
+}
+
+srs_status srs_sim_calculate_efield_time(srs_sim *sim, const double obs[3], double *t, double *e, int64_t *n) {
+  SIM_GUARD(sim);
+  if (!obs || !n) return fail(SRS_ERR_INVALID, "NULL argument");
+  if (srs_status st = sim->ensure_particle()) return st;
+  double dt;
+  int64_t nf, nb;
+  if (srs_status st = srs_trajectory_counts(sim->ctstart, sim->ctstop, sim->particle.t0, sim->npoints, &dt, &nf, &nb))
+    return st;
+  if (!t || !e) {
+    *n = nf + nb;
+    return SRS_OK;
+  }
+  if (*n != nf + nb) return fail(SRS_ERR_INVALID, "output size does not match the trajectory");
+  srs_traj_view v;
+  if (srs_status st = sim->single(sim->particle, v, sim->shoot_for(SRS_PRECISION_FP64))) return st;
+  DeviceBuffer dt_, de;
+  SRS_CUDA(dt_.alloc(sizeof(double) * v.n, sim->stream));
+  SRS_CUDA(de.alloc(sizeof(double) * 3 * v.n, sim->stream));
+  SRS_CUDA(efield_time(v, sim->particle.q, obs, dt_.as<double>(), de.as<double>(), sim->stream));
+  SRS_CUDA(cudaMemcpyAsync(t, dt_.ptr, sizeof(double) * v.n, cudaMemcpyDeviceToHost, sim->stream));
+  SRS_CUDA(cudaMemcpyAsync(e, de.ptr, sizeof(double) * 3 * v.n, cudaMemcpyDeviceToHost, sim->stream));
+  SRS_CUDA(cudaStreamSynchronize(sim->stream));
   return SRS_OK;
 }
 
@@ -670,23 +793,12 @@ int32_t srs_sim_get_nfields(srs_sim *sim) { return sim ? (int32_t)sim->fields.si
 
 srs_status srs_sim_get_bfield(srs_sim *sim, const double *xyz, int64_t np, double *out) {
   SIM_GUARD(sim);
-  if (!xyz || !out || np < 0) return fail(SRS_ERR_INVALID, "bad argument");
-  if (np == 0) return SRS_OK;
-  if (srs_status st = sim->upload_fields()) return st;
-  DeviceBuffer dx, dout;
-  SRS_CUDA(dx.alloc(sizeof(double) * 3 * np, sim->stream));
-  SRS_CUDA(dout.alloc(sizeof(double) * 3 * np, sim->stream));
-  SRS_CUDA(cudaMemcpyAsync(dx.ptr, xyz, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, sim->stream));
-  SRS_CUDA(launch_field_eval(reinterpret_cast<const srs_field *>(sim->d_fields), (int)sim->fields.size(),
-                             dx.as<double>(), np, dout.as<double>(), sim->stream));
-  SRS_CUDA(cudaMemcpyAsync(out, dout.ptr, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost, sim->stream));
-  SRS_CUDA(cudaStreamSynchronize(sim->stream));
-  return SRS_OK;
+  return sim->eval_fields(xyz, np, out, false);
 }
 
 srs_status srs_sim_set_field_grid_data(srs_sim *sim, int32_t k, const double *data, int32_t on_device) {
   SIM_GUARD(sim);
-  if (k < 0 || k >= (int32_t)sim->fields.size() || sim->fields[k].kind != SRS_FIELD_GRID || !data)
+  if (k < 0 || k >= (int32_t)sim->fields.size() || field_shape(sim->fields[k].kind) != SRS_FIELD_GRID || !data)
     return fail(SRS_ERR_INVALID, "field is not a grid");
   const size_t cnt = sim->grid_host[k].size();
   SRS_CUDA(cudaMemcpyAsync(sim->grid_dev[k], data, sizeof(double) * cnt,

@@ -204,13 +204,19 @@ __device__ inline V3 grid_field(const srs_field &f, V3 XIN) {
   return grid_interp(f, f.data, X);
 }
 
-// TFieldContainer::GetF (src/TFieldContainer.cc:92-103): Sum(0,0,0) += each field.
-__device__ inline V3 field_sum(const srs_field *fields, int nfields, V3 X) {
+// kind without the electric flag, and the flag
+__host__ __device__ inline int field_shape(int kind) { return kind & SRS_FIELD_SHAPE_MASK; }
+__host__ __device__ inline bool field_electric(int kind) { return (kind & SRS_FIELD_ELECTRIC) != 0; }
+
+// TFieldContainer::GetF (src/TFieldContainer.cc:92-103): Sum(0,0,0) += each field of the magnetic
+// (electric = false) or the electric container.
+__device__ inline V3 field_sum(const srs_field *fields, int nfields, V3 X, bool electric = false) {
   V3 s = v3(0, 0, 0);
   for (int i = 0; i < nfields; ++i) {
     const srs_field &f = fields[i];
+    if (field_electric(f.kind) != electric) continue;
     V3 b;
-    switch (f.kind) {
+    switch (field_shape(f.kind)) {
       case SRS_FIELD_UNDULATOR: b = undulator_field(f, X); break;
       case SRS_FIELD_GAUSSIAN: b = gaussian_field(f, X); break;
       case SRS_FIELD_UNIFORM_BOX: b = box_field(f, X); break;

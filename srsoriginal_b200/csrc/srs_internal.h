@@ -64,14 +64,21 @@ srs_status read_field_interpolated(std::vector<std::pair<double, std::string>> m
                                    const double *scale, int nscale, srs_field &f, std::vector<double> &data);
 
 // ---- kernel launchers ----
+// Time-domain electric field of one trajectory (first particle of the view) at obs: arrival times (n)
+// and fields (3 n, point-major).
+cudaError_t efield_time(const srs_traj_view &t, double charge, const double obs[3], double *d_t, double *d_e,
+                        cudaStream_t s);
 // Grid samples (doubles) to stage in shared memory for these fields (HOST array): their total, or 0
 // when they do not fit.  Pass it to the RK4 launchers.
 int64_t grid_stage_doubles(const srs_field *host_fields, int nfields);
+// electric: some of the fields are electric (SRS_FIELD_ELECTRIC); has_electric tells from a HOST array
+bool has_electric(const srs_field *host_fields, int nfields);
 cudaError_t launch_rk4(const srs_field *d_fields, int nfields, const srs_particle *d_particles, int nparticles,
                        double dt, int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a,
-                       cudaStream_t s, int64_t stage_doubles);
+                       cudaStream_t s, int64_t stage_doubles, bool electric = false);
 cudaError_t launch_rk4_specs(const srs_field *d_fields, int nfields, const srs_particle *d_particles,
-                             const TrajSpec *d_specs, int nparticles, cudaStream_t s, int64_t stage_doubles);
+                             const TrajSpec *d_specs, int nparticles, cudaStream_t s, int64_t stage_doubles,
+                             bool electric = false);
 // One particle with the serial warp kernel, which returns at once when *d_skip != 0.
 cudaError_t launch_rk4_unless(const srs_field *d_fields, int nfields, const srs_particle *d_particles, double dt,
                               int64_t nfwd, int64_t nbwd, double *d_x, double *d_b, double *d_a, cudaStream_t s,
@@ -84,7 +91,7 @@ cudaError_t launch_rk4_shoot(const srs_field *d_fields, int nfields, const srs_p
                              double *d_b, double *d_a, cudaStream_t s, int64_t stage_doubles, int steps_per_segment,
                              int max_iterations, void *scratch, double *d_stats);
 cudaError_t launch_field_eval(const srs_field *d_fields, int nfields, const double *d_xyz, int64_t np,
-                              double *d_out, cudaStream_t s);
+                              double *d_out, cudaStream_t s, bool electric = false);
 
 // Plain FP64 sums.  Scratch is caller-provided (size from the *_scratch_bytes functions).
 size_t fp64_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles);

@@ -250,6 +250,36 @@ __global__ void total_power_kernel(const double *__restrict__ Bt, const double *
   out[p] = tp;
 }
 
+// The Lienard-Wiechert field of the trajectory point i at the observer and its arrival time
+// (OSCARSSR::CalculateElectricFieldTimeDomain, OSCARSSR.cc:2646-2690; Duke, Synchrotron Radiation, p74):
+//   E = q/(4 pi eps0) (1/(1 - n.beta))^3 [ (1 - beta^2)(n - beta)/R^2 + (1/c) n x ((n - beta) x a/c)/R ],
+//   t = i dt + R/c, in the reference's vector operation order.
+__global__ void efield_time_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
+                                   const double *__restrict__ A, int64_t n, double dt, V3 obs, double C0,
+                                   double *__restrict__ out_t, double *__restrict__ out_e) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V3 x = v3(X[i], X[n + i], X[2 * n + i]);
+  const V3 b = v3(Bt[i], Bt[n + i], Bt[2 * n + i]);
+  const V3 ac = v3(A[i], A[n + i], A[2 * n + i]);
+  const V3 R = obs - x;
+  const double Rm = mag(R);
+  const V3 N = R / Rm;  // TVector3D::UnitVector
+  const double D = Rm;
+  const double Mult = C0 * pow(1.0 / (1.0 - dot(N, b)), 3.0);
+  const V3 nb = N - b;
+  const double s1 = 1.0 - mag2(b);
+  const V3 near = v3(s1 * nb.x, s1 * nb.y, s1 * nb.z) / mag2(R);
+  const V3 c = cross(N, cross(nb, ac));
+  const double ic = 1.0 / kC;
+  const V3 far = v3(ic * c.x, ic * c.y, ic * c.z) / mag(R);
+  const V3 sum = near + far;
+  out_e[3 * i] = Mult * sum.x;
+  out_e[3 * i + 1] = Mult * sum.y;
+  out_e[3 * i + 2] = Mult * sum.z;
+  out_t[i] = (double)i * dt + D / kC;
+}
+
 // Kahan accumulation over particles in order: T3DScalarContainer::AddToPoint (T3DScalarContainer.cc:31-47)
 __global__ void accumulate_kernel(const double *__restrict__ vals, int nparticles, int64_t nout, double w,
                                   double *__restrict__ out, double *__restrict__ comp) {
@@ -363,6 +393,15 @@ cudaError_t accumulate_particles(const double *d_vals, int nparticles, int64_t n
                                  double *d_comp, cudaStream_t s) {
   if (nout <= 0) return cudaSuccess;
   accumulate_kernel<<<blocks_for(nout, 256), 256, 0, s>>>(d_vals, nparticles, nout, weight, d_out, d_comp);
+  return cudaGetLastError();
+}
+
+cudaError_t efield_time(const srs_traj_view &t, double charge, const double obs[3], double *d_t, double *d_e,
+                        cudaStream_t s) {
+  if (t.n <= 0) return cudaSuccess;
+  const double C0 = charge / (four_pi() * kEps0);  // OSCARSSR.cc:2662
+  efield_time_kernel<<<(unsigned)((t.n + 127) / 128), 128, 0, s>>>(t.x, t.beta, t.aoc, t.n, t.dt, ld3(obs), C0, d_t,
+                                                                    d_e);
   return cudaGetLastError();
 }
 

@@ -218,6 +218,66 @@ class sr:  # noqa: N801  (the reference's type name)
         check(lib.srs_sim_get_bfield(self._h, dptr(pts), 1, dptr(out)))
         return [float(out[0]), float(out[1]), float(out[2])]
 
+    # ------------------------------------------------------------ electric fields
+    def add_efield_file(self, ifile, iformat, rotations=None, translation=None, scale=None):
+        """An electric field map file (OSCARSSR_Python.cc:876-935); like the reference, scale is accepted
+        and not applied."""
+        if not ifile or not iformat:
+            raise ValueError("'ifile' or 'iformat' is blank")
+        rot = _opt3(rotations, "rotations")
+        tr = _opt3(translation, "translation")
+        st = lib.srs_sim_add_efield_file(self._h, str(ifile).encode(), str(iformat).encode(), v3(rot), v3(tr))
+        if st != _lib.SRS_OK:
+            raise ValueError("Could not import electric field.  Check 'ifile' and 'iformat' are correct")
+
+    def add_efield_gaussian(self, efield, sigma, rotations=None, translation=None):
+        e = _list3(efield, "efield")
+        s = _list3(sigma, "sigma")
+        check(lib.srs_sim_add_efield_gaussian(self._h, v3(e), v3(s), v3(_opt3(rotations, "rotations")),
+                                              v3(_opt3(translation, "translation"))))
+
+    def add_efield_uniform(self, efield, width=None, rotations=None, translation=None):
+        e = _list3(efield, "efield")
+        w = _opt3(width, "width")
+        check(lib.srs_sim_add_efield_uniform(self._h, v3(e), v3(w), v3(_opt3(rotations, "rotations")),
+                                             v3(_opt3(translation, "translation"))))
+
+    def add_efield_undulator(self, efield, period, nperiods, phase=0.0, rotations=None, translation=None):
+        e = _list3(efield, "efield")
+        p = _list3(period, "period")
+        check(lib.srs_sim_add_efield_undulator(self._h, v3(e), v3(p), int(nperiods), float(phase),
+                                               v3(_opt3(rotations, "rotations")),
+                                               v3(_opt3(translation, "translation"))))
+
+    def add_field_gaussian(self, sigma, bfield=None, efield=None, rotations=None, translation=None):
+        """A Gaussian electric field (OSCARSSR_Python.cc:1306-1390); as in the reference, a 'bfield' here
+        adds nothing (its call is disabled there)."""
+        has_b, has_e = bool(bfield) and len(bfield) > 0, bool(efield) and len(efield) > 0
+        if has_b and has_e:
+            raise ValueError("You cannot define both 'bfield' and 'efield'")
+        if has_b:
+            _list3(bfield, "bfield")
+        elif has_e:
+            e = _list3(efield, "efield")
+        else:
+            raise ValueError("You must define either 'bfield' or 'efield'")
+        s = _list3(sigma, "sigma")
+        rot = _opt3(rotations, "rotations")
+        tr = _opt3(translation, "translation")
+        if has_e:
+            check(lib.srs_sim_add_efield_gaussian(self._h, v3(e), v3(s), v3(rot), v3(tr)))
+
+    def get_efield(self, x):
+        if not isinstance(x, list) or len(x) != 3:
+            raise ValueError("Incorrect format in 'rotations'")
+        pts = np.ascontiguousarray(np.array(x, dtype=np.float64))
+        out = np.zeros(3)
+        check(lib.srs_sim_get_efield(self._h, dptr(pts), 1, dptr(out)))
+        return [float(out[0]), float(out[1]), float(out[2])]
+
+    def clear_efields(self):
+        check(lib.srs_sim_clear_efields(self._h))
+
     def clear_bfields(self):
         check(lib.srs_sim_clear_bfields(self._h))
 
@@ -632,6 +692,25 @@ class sr:  # noqa: N801  (the reference's type name)
         return xyz, out
 
     # ------------------------------------------------------------ total power
+    def calculate_efield_vs_time(self, obs, ofile=""):
+        """The electric field at obs in the time domain (OSCARSSR_Python.cc:3573-3640,
+        OSCARSSR.cc:2646-2690): [[t, [Ex, Ey, Ez]], ...] for every trajectory point in time order; the
+        arrival times are not evenly spaced.  ofile gets "Ex Ey Ez t" lines, the reference's dim-3 scalar
+        format."""
+        if lib.srs_sim_get_nparticle_beams(self._h) < 1:
+            raise ValueError("No particle beam defined")
+        o = _list3(obs, "obs")
+        n = C.c_int64(0)
+        check(lib.srs_sim_calculate_efield_time(self._h, dptr(np.array(o)), None, None, C.byref(n)))
+        t, e = np.zeros(n.value), np.zeros(3 * n.value)
+        check(lib.srs_sim_calculate_efield_time(self._h, dptr(np.array(o)), dptr(t), dptr(e), C.byref(n)))
+        e = e.reshape(-1, 3)
+        if ofile:
+            with open(ofile, "w") as f:
+                for ee, tt in zip(e, t):
+                    f.write(f"{ee[0]:.6e} {ee[1]:.6e} {ee[2]:.6e} {tt:.6e}\n")
+        return [[float(tt), [float(ee[0]), float(ee[1]), float(ee[2])]] for tt, ee in zip(t, e)]
+
     def calculate_total_power(self):
         """Total radiated power [W] of the current particle (OSCARSSR.cc:1939-1978)."""
         if lib.srs_sim_get_nparticle_beams(self._h) < 1:

@@ -510,9 +510,71 @@ def field_files():
     save("field_files.npz", **out)
 
 
+def efield():
+    """Electric fields (OSCARSSR_Python.cc:876-1390, OSCARSSR.cc:690-793) in the RK4, their evaluation,
+    the time-domain field (OSCARSSR.cc:2646-2690), and the disabled magnetic add_field_gaussian."""
+    out = {}
+    rng = np.random.default_rng(13)
+    pts = np.column_stack([rng.uniform(-0.01, 0.01, 50), rng.uniform(-0.01, 0.01, 50), rng.uniform(-1.0, 1.0, 50)])
+    out["points"] = pts
+
+    def setup(o, n):
+        W.setup_beam(o, n)
+
+    # E only: a uniform box and a rotated Gaussian
+    o = new_sr()
+    setup(o, 4001)
+    o.add_efield_uniform(efield=[3e6, 0, 0], width=[0, 0, 0.5])
+    o.add_efield_gaussian(efield=[0, 5e6, 1e5], sigma=[0.02, 0.0, 0.1], translation=[0, 0, 0.5],
+                          rotations=[0.0, 0.01, 0.0])
+    X, B = traj_arrays(o.calculate_trajectory())
+    out["e_only_x"], out["e_only_beta"] = X, B
+    out["e_only_efield"] = np.array([o.get_efield(list(map(float, p))) for p in pts])
+    out["e_only_bfield"] = np.array([o.get_bfield(list(map(float, p))) for p in pts])
+    r = o.calculate_efield_vs_time(obs=[0, 0, 30])
+    out["e_only_t"] = np.array([q[0] for q in r])
+    out["e_only_e"] = np.array([q[1] for q in r])
+    # E and B: an undulator and an electric undulator with a phase
+    o = new_sr()
+    setup(o, 8001)
+    W.setup_undulator(o)
+    o.add_efield_undulator(efield=[0, 2e7, 0], period=[0, 0, W.PERIOD], nperiods=W.NPERIODS, phase=0.3)
+    X, B = traj_arrays(o.calculate_trajectory())
+    out["eb_x"], out["eb_beta"] = X, B
+    out["eb_efield"] = np.array([o.get_efield(list(map(float, p))) for p in pts])
+    sp = o.calculate_spectrum(obs=[0, 0, 30], npoints=20, energy_range_eV=[140, 160], nthreads=NT)
+    out["eb_spectrum"] = np.array(sp)
+    r = o.calculate_efield_vs_time(obs=[0.001, 0, 30])
+    out["eb_t"] = np.array([q[0] for q in r])
+    out["eb_e"] = np.array([q[1] for q in r])
+    # clearing one container keeps the other
+    o.clear_bfields()
+    out["eb_cleared_b_efield"] = np.array([o.get_efield(list(map(float, p))) for p in pts[:5]])
+    # the magnetic add_field_gaussian adds nothing; the electric one adds a Gaussian
+    o = new_sr()
+    setup(o, 2001)
+    o.add_field_gaussian(sigma=[0, 0, 0.1], bfield=[0, 1.0, 0])
+    X, _ = traj_arrays(o.calculate_trajectory())
+    out["fg_b_x"] = X
+    o.add_field_gaussian(sigma=[0, 0, 0.1], efield=[1e6, 0, 0])
+    out["fg_e_efield"] = np.array([o.get_efield(list(map(float, p))) for p in pts[:5]])
+    errs = {}
+    for key, call in (("fg_both", lambda: o.add_field_gaussian(sigma=[0, 0, 1], bfield=[0, 1, 0], efield=[1, 0, 0])),
+                      ("fg_none", lambda: o.add_field_gaussian(sigma=[0, 0, 1])),
+                      ("efield_format", lambda: o.add_efield_uniform(efield=[1, 0]))):
+        try:
+            call()
+            errs[key] = None
+        except ValueError as exc:
+            errs[key] = str(exc)
+    with open(os.path.join(HERE, "efield_errors.json"), "w") as fh:
+        json.dump(errs, fh, indent=1)
+    save("efield.npz", **out)
+
+
 if __name__ == "__main__":
     parts = sys.argv[1:] or ["cfg0", "cfg1", "cfg2", "misc", "beam", "beam32", "points", "grid", "adjoint",
-                             "quirks", "aggregate", "fieldfiles"]
+                             "quirks", "aggregate", "fieldfiles", "efield"]
     if "cfg0" in parts:
         e1 = cfg0()
         print("E1 (first-harmonic peak of the config-0 spectrum):", repr(e1))
@@ -523,6 +585,7 @@ if __name__ == "__main__":
     for name, fn in (("cfg2", cfg2), ("misc", misc), ("beam", beam), ("beam32", beam32), ("points", points_surface),
                      ("grid", grid),
                      ("adjoint", adjoint),
-                     ("quirks", quirks), ("aggregate", aggregate), ("fieldfiles", field_files)):
+                     ("quirks", quirks), ("aggregate", aggregate), ("fieldfiles", field_files),
+                     ("efield", efield)):
         if name in parts:
             fn()
