@@ -14,7 +14,6 @@ namespace srs {
 namespace tiles {
 
 constexpr int kThreads = 128;
-constexpr int kTileA = 8, kTileB = 16;  // points of a CTA tile along u1 and u2 (kTileA * kTileB == kThreads)
 constexpr int kSub = 128;               // trajectory points per shared-memory tile
 constexpr int kEnergiesPerThread = 4;
 
@@ -58,10 +57,75 @@ inline int64_t wave_slots(K kernel) {
   return (int64_t)sms * occ;
 }
 
-struct GridTiles {
-  int t1, t2;  // tiles along n1 and n2
+// Observation-grid tiles.  The u2 axis is cut into strips of balanced width (8 to 16 points when the
+// grid is that wide), the points of a strip are taken row by row (u1 outer), and a CTA covers up to
+// kThreads consecutive points of one strip: a compact block of at most 17 rows whose idle lanes are
+// those of the last tile of each strip.  (A 101 x 101 map: 84 tiles with 5 % idle lanes, where
+// rectangles of 8 x 16 points need 91 tiles with 12 % idle.)
+struct StripTiles {
+  int n1, n2;
+  int wn, nwide;              // strips [0, nwide) are wn + 1 points wide, the others wn
+  int per_wide, per_narrow;   // tiles per strip of each width
+  int tiles;
 };
-inline GridTiles tiles_of(const srs_grid2d &g) { return GridTiles{(g.n1 + kTileA - 1) / kTileA, (g.n2 + kTileB - 1) / kTileB}; }
+
+// Points of one tile of a strip w points wide: kThreads, or 16 rows of a narrower strip.
+__host__ __device__ inline int strip_tile_points(int w) { return 16 * w < kThreads ? 16 * w : kThreads; }
+
+inline StripTiles strip_tiles(int n1, int n2) {
+  StripTiles best{};
+  const int lo = std::max(1, (n2 + 15) / 16), hi = std::max(lo, n2 / 8);
+  for (int ns = lo; ns <= hi; ++ns) {
+    StripTiles m{};
+    m.n1 = n1;
+    m.n2 = n2;
+    m.wn = n2 / ns;
+    m.nwide = n2 % ns;
+    auto per = [&](int w) {
+      const int64_t p = strip_tile_points(w);
+      return (int)(((int64_t)n1 * w + p - 1) / p);
+    };
+    m.per_wide = per(m.wn + 1);
+    m.per_narrow = per(m.wn);
+    m.tiles = m.nwide * m.per_wide + (ns - m.nwide) * m.per_narrow;
+    if (ns == lo || m.tiles < best.tiles) best = m;
+  }
+  return best;
+}
+inline StripTiles strip_tiles(const srs_grid2d &g) { return strip_tiles(g.n1, g.n2); }
+
+// Thread tid's grid point (i1, i2) in tile `tile`, whether it holds one, and the tile's anchor point
+// (ca, cb): the middle row of the tile's points and the middle column of its strip.
+struct TilePoint {
+  int i1, i2, ca, cb;
+  bool active;
+};
+__host__ __device__ inline TilePoint strip_point(const StripTiles &m, int tile, int tid) {
+  const int wide_tiles = m.nwide * m.per_wide;
+  int w, c0, t;
+  if (tile < wide_tiles) {
+    const int s = tile / m.per_wide;
+    t = tile - s * m.per_wide;
+    w = m.wn + 1;
+    c0 = s * w;
+  } else {
+    const int r = tile - wide_tiles, s = r / m.per_narrow;
+    t = r - s * m.per_narrow;
+    w = m.wn;
+    c0 = m.nwide * (m.wn + 1) + s * w;
+  }
+  const int pts = strip_tile_points(w);
+  const int64_t q0 = (int64_t)t * pts, qn = (int64_t)m.n1 * w;
+  const int64_t qend = q0 + pts < qn ? q0 + pts : qn;
+  const int64_t q = q0 + tid;
+  TilePoint P;
+  P.active = tid < pts && q < qend;
+  P.i1 = (int)(q / w);
+  P.i2 = c0 + (int)(q % w);
+  P.ca = (int)((q0 / w + (qend - 1) / w) / 2);
+  P.cb = c0 + w / 2;
+  return P;
+}
 
 // FP64 anchor common to flux and power density: the tile centre as seen from trajectory point i.
 struct Anchor {
@@ -98,130 +162,141 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 
-// Per trajectory point, 13 FP32 values anchored at the tile centre, stored for PAIRS of consecutive
-// points: record g of pair q is (field 2g of point 2q, of point 2q+1, field 2g+1 of 2q, of 2q+1), so
-// one 16-byte broadcast load yields two fields of both points, ready for the packed instructions.
-//   0 phase (turns, mod 1)        1 k1 (turns per grid step along u1, mod 1)
-//   2 k2 (along u2)               3 (w/c)/(2 D_c)/2pi (turns per m^2)
-//   4-6 n_c                       7 1/(2 D_c)
-//   8 1/D_c                       9-11 (n_c - bhat) + bhat (1 - |beta|)
-//   12 near-field z term -(c/w) n_cz / D_c^2          (13: padding)
+// Per trajectory point, 14 FP32 values anchored at the tile's anchor point, stored for PAIRS of
+// consecutive points: record g of pair q is (field 2g of point 2q, of point 2q+1, field 2g+1 of 2q,
+// of 2q+1), so one 16-byte broadcast load yields two fields of both points, ready for the packed
+// instructions.  Signs are chosen so that the inner loop needs no negation.
+//   0 phase (turns, mod 1)                        1 k1 (turns per grid step along u1, mod 1)
+//   2 k2 (along u2)                               3 -(w/c)/(2 D_c)/2pi (turns per m^2)
+//   4-6 n_c                                       7 1/(2 D_c)
+//   8 1/D_c                                       9 1/D_c^2
+//   10-12 (n_c - bhat) + bhat (1 - |beta|)        13 near-field z term -(c/w) n_cz / D_c^2
 constexpr int kFluxFields = 14;
 struct FluxShared {
-  float4 r[kFluxFields / 2][kSub / 2];
+  float4 r[2][kFluxFields / 2][kSub / 2];  // double-buffered: sub-tile k in r[k & 1]
 };
 
-// Flux: one tile of kTileA x kTileB grid points (tile T1, T2) against trajectory points [i0, iend);
-// writes the six partial sums (Re/Im of E_x, E_y, E_z without the final constant) of every point of
-// the tile to out6[c * np + j].
+// Flux: one strip tile (tile index `tile` of map m) against trajectory points [i0, iend); writes the six
+// partial sums (Re/Im of E_x, E_y, E_z without the final constant) of every point of the tile to
+// out6[c * np + j].
 __device__ __forceinline__ void flux_tile(const double *__restrict__ xp, const double *__restrict__ bp, int64_t n,
-                                          double dt, const srs_grid2d &g, double omega, int T1, int T2, int64_t i0,
-                                          int64_t iend, double *__restrict__ out6, FluxShared &sh) {
-  // Phases are kept in turns so that the reduction to [-1/2, 1/2) is exact (x - rint(x), rint by
-  // the 1.5 * 2^23 shift, exact for |x| < 2^22 turns).
-  // Terms below FP32 resolution are dropped: the third-order distance term g (|Delta|^2 - g^2)/(2 D_c^2)
-  // (< 1e-7 rad here) and the near-field term's x, y parts (relative size lambda/(2 pi D) times
-  // n_perp, < 1e-10 at 30 m); 1/D_j = (1/D_c)(1 - (D_j - D_c)/D_c) to first order (relative error
-  // ((D_j - D_c)/D_c)^2 < 1e-16).
-  float *rec = &sh.r[0][0].x;
+                                          double dt, const srs_grid2d &g, const StripTiles &m, double omega,
+                                          int tile, int64_t i0, int64_t iend, double *__restrict__ out6,
+                                          FluxShared &sh) {
+  // Expansion about the anchor point O_c (distance D_c, direction n_c from trajectory point i) for
+  // the grid point O_c + Delta: with g = n_c . Delta and h = |Delta|^2 - g^2,
+  //   D_j - D_c = g + h/(2 D_c)  (the third-order term g h/(2 D_c^2), < 1e-7 rad here, is dropped),
+  //   1/D_j = (1/D_c)(1 - (D_j - D_c)/D_c)  (relative error ((D_j - D_c)/D_c)^2 < 1e-16),
+  //   phase = w tau_c + k1 da + k2 db + (w/c) h/(2 D_c),
+  // and the near-field term keeps its z part (its x, y parts are lambda/(2 pi D) times n_perp, < 1e-10
+  // at 30 m).  Phases are kept in turns: the per-point phases and the grid-step phases k1, k2 are
+  // reduced in FP64, and the FP32 phase of a tile point is reduced exactly (x - rint(x), rint by the
+  // 1.5 * 2^23 shift, exact for |x| < 2^22 turns) before __sincosf.
   const int tid = threadIdx.x;
-  const int a = tid / kTileB, b = tid % kTileB;
-  const int i1 = T1 * kTileA + a, i2 = T2 * kTileB + b;
-  const bool active = i1 < g.n1 && i2 < g.n2;
-  const int64_t j = (int64_t)i1 * g.n2 + i2;
-  const int64_t np = (int64_t)g.n1 * g.n2;
-  // tile centre (a grid point) and this thread's integer offsets from it
-  const int ca = T1 * kTileA + kTileA / 2, cb = T2 * kTileB + kTileB / 2;
-  double Oc[3];
-  for (int c = 0; c < 3; ++c) Oc[c] = g.origin[c] + (double)ca * g.u1[c] + (double)cb * g.u2[c];
-  const int da = i1 - ca, db = i2 - cb;
-  float Dl[3];
-  for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);
-  const float2 Dx = f2(Dl[0], Dl[0]), Dy = f2(Dl[1], Dl[1]), Dz = f2(Dl[2], Dl[2]);
-  const float ddv = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
-  const float2 dd = f2(ddv, ddv), fda = f2((float)da, (float)da), fdb = f2((float)db, (float)db);
-  const float2 shift = f2(12582912.0f, 12582912.0f), two_pi = f2(6.28318530717958647692f, 6.28318530717958647692f);
+  const TilePoint P = strip_point(m, tile, tid);
+  const bool active = P.active;
+  const int da = P.i1 - P.ca, db = P.i2 - P.cb;
   const double wc = omega / kC;
-  const double inv2pi = 0.15915494309189535;
   double E[6] = {0, 0, 0, 0, 0, 0};
 
-  // slot of field f of point t (t < kSub) in the pair-packed records
-  auto put = [&](int t, int f, float v) { rec[((f >> 1) * (kSub / 2) + (t >> 1)) * 4 + (f & 1) * 2 + (t & 1)] = v; };
-
-  for (int64_t base = i0; base < iend; base += kSub) {
+  // the records of trajectory points [base, base + kSub) into buffer b
+  auto fill = [&](int b, int64_t base) {
+    float *rec = &sh.r[b][0][0].x;
+    auto put = [&](int t, int f, float v) { rec[((f >> 1) * (kSub / 2) + (t >> 1)) * 4 + (f & 1) * 2 + (t & 1)] = v; };
     const int cnt = (int)imin64(kSub, iend - base);
-    __syncthreads();
     if (tid < cnt) {
       const int64_t i = base + tid;
+      double Oc[3];
+      for (int c = 0; c < 3; ++c) Oc[c] = g.origin[c] + (double)P.ca * g.u1[c] + (double)P.cb * g.u2[c];
       const Anchor A = make_anchor(Oc, xp, bp, n, i);
       const double tau = dt * (double)i + A.Dc / kC;
-      const double k1 = reduce_2pi(wc * (A.nc[0] * g.u1[0] + A.nc[1] * g.u1[1] + A.nc[2] * g.u1[2]));
-      const double k2 = reduce_2pi(wc * (A.nc[0] * g.u2[0] + A.nc[1] * g.u2[1] + A.nc[2] * g.u2[2]));
+      const double inv2pi = 0.15915494309189535;  // 1/(2 pi)
       put(tid, 0, (float)(reduce_2pi(omega * tau) * inv2pi));
-      put(tid, 1, (float)(k1 * inv2pi));
-      put(tid, 2, (float)(k2 * inv2pi));
-      put(tid, 3, (float)(wc * 0.5 * A.invDc * inv2pi));
+      put(tid, 1, (float)(reduce_2pi(wc * (A.nc[0] * g.u1[0] + A.nc[1] * g.u1[1] + A.nc[2] * g.u1[2])) * inv2pi));
+      put(tid, 2, (float)(reduce_2pi(wc * (A.nc[0] * g.u2[0] + A.nc[1] * g.u2[1] + A.nc[2] * g.u2[2])) * inv2pi));
+      put(tid, 3, (float)(-wc * 0.5 * A.invDc * inv2pi));
       put(tid, 4, (float)A.nc[0]);
       put(tid, 5, (float)A.nc[1]);
       put(tid, 6, (float)A.nc[2]);
       put(tid, 7, (float)(0.5 * A.invDc));
       put(tid, 8, (float)A.invDc);
-      put(tid, 9, (float)(A.dc[0] + A.bhat[0] * A.omb));
-      put(tid, 10, (float)(A.dc[1] + A.bhat[1] * A.omb));
-      put(tid, 11, (float)(A.dc[2] + A.bhat[2] * A.omb));
-      put(tid, 12, (float)(-(kC / omega) * A.invDc * A.invDc * A.nc[2]));
+      put(tid, 9, (float)(A.invDc * A.invDc));
+      put(tid, 10, (float)(A.dc[0] + A.bhat[0] * A.omb));
+      put(tid, 11, (float)(A.dc[1] + A.bhat[1] * A.omb));
+      put(tid, 12, (float)(A.dc[2] + A.bhat[2] * A.omb));
+      put(tid, 13, (float)(-(kC / omega) * A.invDc * A.invDc * A.nc[2]));
     } else if (tid == cnt && (cnt & 1)) {
       // the odd count's partner slot: all zero, so 1/D_j = 0 and its amplitude and near-field term vanish
-      for (int f = 0; f < 13; ++f) put(tid, f, 0.0f);
+      for (int f = 0; f < kFluxFields; ++f) put(tid, f, 0.0f);
     }
+  };
+
+  __syncthreads();  // the caller's previous use of sh is over
+  if (i0 < iend) fill(0, i0);
+  int b = 0;
+  for (int64_t base = i0; base < iend; base += kSub, b ^= 1) {
+    const int cnt = (int)imin64(kSub, iend - base);
+    // records of this sub-tile complete; every thread is done with the other buffer
     __syncthreads();
+    if (base + kSub < iend) fill(b ^ 1, base + kSub);
     if (!active) continue;
+    // this thread's offset from the anchor point (formed here, after the FP64 anchors, so that it does
+    // not occupy registers while they are computed)
+    float Dl[3];
+    for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);
+    const float2 Dx = f2(Dl[0], Dl[0]), Dy = f2(Dl[1], Dl[1]), Dz = f2(Dl[2], Dl[2]);
+    const float2 Dxn = f2(-Dl[0], -Dl[0]), Dyn = f2(-Dl[1], -Dl[1]), Dzn = f2(-Dl[2], -Dl[2]);
+    const float ddv = -(Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2]);
+    const float2 ddn = f2(ddv, ddv), fda = f2((float)da, (float)da), fdb = f2((float)db, (float)db);
+    const float2 shift = f2(12582912.0f, 12582912.0f), nshift = f2(-12582912.0f, -12582912.0f),
+                 mone = f2(-1.0f, -1.0f), two_pi = f2(6.28318530717958647692f, 6.28318530717958647692f);
+    // The accumulators collect minus the field: the sum over points of amp (cos, sin) with amp =
+    // ((n_c - bhat + bhat omb) + (Delta - n_c del)/D_j)/D_j, and for z of (amp - i nf)(cos + i sin).
     float2 acc[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) acc[c] = f2(0.f, 0.f);
     const int pairs = (cnt + 1) >> 1;
+    const float4(*r)[kSub / 2] = sh.r[b];
 #pragma unroll 2
     for (int q = 0; q < pairs; ++q) {
-      const float4 R0 = sh.r[0][q], R1 = sh.r[1][q], R2 = sh.r[2][q], R3 = sh.r[3][q], R4 = sh.r[4][q],
-                   R5 = sh.r[5][q], R6 = sh.r[6][q];
-      const float2 ph0 = f2(R0.x, R0.y), k1 = f2(R0.z, R0.w), k2 = f2(R1.x, R1.y), qc = f2(R1.z, R1.w);
+      const float4 R0 = r[0][q], R1 = r[1][q], R2 = r[2][q], R3 = r[3][q], R4 = r[4][q], R5 = r[5][q],
+                   R6 = r[6][q];
+      const float2 ph0 = f2(R0.x, R0.y), k1 = f2(R0.z, R0.w), k2 = f2(R1.x, R1.y), qcn = f2(R1.z, R1.w);
       const float2 nx = f2(R2.x, R2.y), ny = f2(R2.z, R2.w), nz = f2(R3.x, R3.y), hinv = f2(R3.z, R3.w);
-      const float2 w = f2(R4.x, R4.y), bx = f2(R4.z, R4.w), by = f2(R5.x, R5.y), bz = f2(R5.z, R5.w);
-      const float2 nf = f2(R6.x, R6.y);
-      const float2 gq = fma2(nz, Dz, fma2(ny, Dy, mul2(nx, Dx)));  // n_c . Delta
-      const float2 h = fma2(neg2(gq), gq, dd);                     // |Delta|^2 - g^2
-      const float2 del = fma2(h, hinv, gq);                        // D_j - D_c
-      const float2 t = mul2(del, w);
-      const float2 rinv = fma2(neg2(t), w, w);                     // 1/D_j
+      const float2 w = f2(R4.x, R4.y), w2 = f2(R4.z, R4.w), bx = f2(R5.x, R5.y), by = f2(R5.z, R5.w);
+      const float2 bz = f2(R6.x, R6.y), nf = f2(R6.z, R6.w);
+      const float2 gqn = fma2(nz, Dzn, fma2(ny, Dyn, mul2(nx, Dxn)));  // -g
+      const float2 hn = fma2(gqn, gqn, ddn);                          // -h
+      const float2 deln = fma2(hn, hinv, gqn);                        // D_c - D_j
+      const float2 rinv = fma2(deln, w2, w);                          // 1/D_j
       float2 ph = fma2(k1, fda, ph0);
       ph = fma2(k2, fdb, ph);
-      ph = fma2(h, qc, ph);                                        // turns
-      const float2 fr = add2(ph, neg2(add2(add2(ph, shift), neg2(shift))));
-      const float2 x = mul2(fr, two_pi);
+      ph = fma2(hn, qcn, ph);                                         // turns
+      const float2 rn = add2(add2(ph, shift), nshift);                 // rint(ph)
+      const float2 x = mul2(fma2(rn, mone, ph), two_pi);              // rad, in [-pi, pi]
       float2 sn, cs;
       __sincosf(x.x, &sn.x, &cs.x);
       __sincosf(x.y, &sn.y, &cs.y);
-      // minus the amplitude: ((n_c - bhat + bhat omb) + (Delta - n_c del)/D_j)/D_j
-      const float2 ax = mul2(fma2(fma2(neg2(nx), del, Dx), rinv, bx), rinv);
-      const float2 ay = mul2(fma2(fma2(neg2(ny), del, Dy), rinv, by), rinv);
-      const float2 az = mul2(fma2(fma2(neg2(nz), del, Dz), rinv, bz), rinv);
-      acc[0] = fma2(neg2(ax), cs, acc[0]);
-      acc[1] = fma2(neg2(ax), sn, acc[1]);
-      acc[2] = fma2(neg2(ay), cs, acc[2]);
-      acc[3] = fma2(neg2(ay), sn, acc[3]);
-      acc[4] = fma2(neg2(az), cs, fma2(neg2(nf), sn, acc[4]));
-      acc[5] = fma2(neg2(az), sn, fma2(nf, cs, acc[5]));
+      const float2 ax = mul2(fma2(fma2(nx, deln, Dx), rinv, bx), rinv);
+      const float2 ay = mul2(fma2(fma2(ny, deln, Dy), rinv, by), rinv);
+      const float2 az = mul2(fma2(fma2(nz, deln, Dz), rinv, bz), rinv);
+      acc[0] = fma2(ax, cs, acc[0]);
+      acc[1] = fma2(ax, sn, acc[1]);
+      acc[2] = fma2(ay, cs, acc[2]);
+      acc[3] = fma2(ay, sn, acc[3]);
+      acc[4] = fma2(az, cs, fma2(nf, sn, acc[4]));
+      acc[5] = fma2(az, sn, fma2(neg2(nf), cs, acc[5]));
     }
 #pragma unroll
-    for (int c = 0; c < 6; ++c) E[c] += (double)acc[c].x + (double)acc[c].y;
+    for (int c = 0; c < 6; ++c) E[c] -= (double)acc[c].x + (double)acc[c].y;
   }
   if (active) {
-    double *o = out6 + j;
+    const int64_t np = (int64_t)g.n1 * g.n2;
+    double *o = out6 + (int64_t)P.i1 * g.n2 + P.i2;
 #pragma unroll
     for (int c = 0; c < 6; ++c) o[c * np] = E[c];
   }
 }
-
 
 // ---- flux at an arbitrary list of observation points ----
 //

@@ -2,7 +2,7 @@
 //
 // Jobs of very different sizes (a 64-point map next to a 40401-point one, 100 energies next to 4000,
 // trajectories of 5001 to 40001 points) are cut into items of the same shape as the one-shot mixed
-// kernels' CTAs -- a tile of 8 x 16 grid points or 512 energies against one chunk of the trajectory.
+// kernels' CTAs -- a tile of up to 128 grid points or 512 energies against one chunk of the trajectory.
 // The host orders the items by decreasing cost (longest-processing-time first), and a grid of
 // resident CTAs (one wave: SMs x CTAs per SM) drains them: each CTA takes the next item with one
 // atomicAdd on a ticket and runs it.  No CTA waits on another (no spin), so the launch always ends.
@@ -31,7 +31,7 @@ using namespace tiles;
 
 struct QJob {
   int kind;
-  int t2;          // flux: tiles along n2
+  StripTiles tiles;  // flux: the map's tiles
   int64_t chunk;   // trajectory points per item
   const double *x, *beta;
   int64_t n;
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kThreads) queue_kernel(const QJob *__restrict_
     const int64_t i0 = (int64_t)w.chunk * J.chunk, i1 = imin64(J.n, i0 + J.chunk);
     double *out6 = J.partial + (int64_t)w.chunk * 6 * J.nout;
     if (J.kind == SRS_JOB_FLUX)
-      flux_tile(J.x, J.beta, J.n, J.dt, J.g, J.omega, w.tile / J.t2, w.tile % J.t2, i0, i1, out6, sh.f);
+      flux_tile(J.x, J.beta, J.n, J.dt, J.g, J.tiles, J.omega, w.tile, i0, i1, out6, sh.f);
     else
       spectrum_tile(J.x, J.beta, J.n, J.dt, J.obs, J.omegas, J.ne, w.tile, i0, i1, out6, sh.s);
   }
@@ -175,10 +175,10 @@ srs_status srs_queue_create(srs_queue **out, const srs_job *jobs, int32_t njobs,
         return fail(SRS_ERR_INVALID, "job " + std::to_string(j) + ": bad flux grid or energy");
       J.g = s.grid;
       J.omega = ev_to_omega(s.energy_ev);
-      J.t2 = (s.grid.n2 + kTileB - 1) / kTileB;
-      ntiles = ((s.grid.n1 + kTileA - 1) / kTileA) * J.t2;
+      J.tiles = strip_tiles(s.grid);
+      ntiles = J.tiles.tiles;
       J.nout = (int64_t)s.grid.n1 * s.grid.n2;
-      per_item = kTileA * kTileB;
+      per_item = kThreads;
       q->evals += (double)J.nout * s.traj.n;
     } else if (s.kind == SRS_JOB_SPECTRUM) {
       if (s.ne < 1 || !s.d_energies) return fail(SRS_ERR_INVALID, "job " + std::to_string(j) + ": no energies");

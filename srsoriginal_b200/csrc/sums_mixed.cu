@@ -43,16 +43,16 @@ namespace {
 
 // ---------------------------------------------------------------- flux on a grid
 
-__global__ void __launch_bounds__(kThreads) flux_mixed_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
-                                                              int64_t n, double dt, srs_grid2d g, double omega,
-                                                              int64_t chunk, double *__restrict__ partial) {
+__global__ void __launch_bounds__(kThreads, 6) flux_mixed_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
+                                                              int64_t n, double dt, srs_grid2d g, StripTiles m,
+                                                              double omega, int64_t chunk,
+                                                              double *__restrict__ partial) {
   __shared__ tiles::FluxShared sh;
-  const int nt2 = (g.n2 + kTileB - 1) / kTileB;
   const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
   const int64_t np = (int64_t)g.n1 * g.n2;
   const int64_t i0 = (int64_t)s * chunk;
-  tiles::flux_tile(X + (int64_t)p * 3 * n, Bt + (int64_t)p * 3 * n, n, dt, g, omega, blockIdx.x / nt2,
-                   blockIdx.x % nt2, i0, imin64(n, i0 + chunk), partial + ((int64_t)p * S + s) * 6 * np, sh);
+  tiles::flux_tile(X + (int64_t)p * 3 * n, Bt + (int64_t)p * 3 * n, n, dt, g, m, omega, blockIdx.x, i0,
+                   imin64(n, i0 + chunk), partial + ((int64_t)p * S + s) * 6 * np, sh);
 }
 
 // ---------------------------------------------------------------- flux at a list of points
@@ -73,55 +73,45 @@ __global__ void __launch_bounds__(kThreads) flux_points_mixed_kernel(const doubl
 
 __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__restrict__ X, const double *__restrict__ Bt,
                                                             const double *__restrict__ Ac, int64_t n, srs_grid2d g,
-                                                            double nx_, double ny_, double nz_, int directional,
-                                                            int64_t chunk, double *__restrict__ partial) {
+                                                            StripTiles m, double nx_, double ny_, double nz_,
+                                                            int directional, int64_t chunk,
+                                                            double *__restrict__ partial) {
   // (1 - n.beta)^5 ~ 1e-39 does not fit FP32, so the FP32 term is scaled: with omb = 1 - |beta|,
   // 1 - n.beta = omb_i * opn, opn = 1 + (|beta|/(2 omb_i)) |n - bhat|^2 >= 1, and
   // 1/(1 - n.beta)^5 = (omb_ref/omb_i)^5 / opn^5 / omb_ref^5; the last factor (~1e39) is applied in FP64.
-  // Per trajectory point, 19 FP32 values anchored at the tile centre, stored for pairs of consecutive
-  // points as in the flux tile (record g of pair q = fields 2g, 2g+1 of both points):
+  // Per trajectory point, 20 FP32 values anchored at the tile's anchor point, stored for pairs of
+  // consecutive points as in the flux tile (record g of pair q = fields 2g, 2g+1 of both points), with
+  // signs chosen so that the inner loop needs no negation:
   //   0-2 n_c        3 1/D_c        4-6 n_c - bhat      7 1/(2 D_c)
-  //   8-10 bhat (1 - |beta|)        11 omb_i = 1 - |beta_i|
+  //   8-10 bhat (1 - |beta|)        11 -omb_i = -(1 - |beta_i|)
   //   12-14 a/c      15 |beta|/(2 omb_i)                16 bhat . a/c
-  //   17 (omb_ref/omb_i)^5          18 n_c . normal     (19: padding)
+  //   17 (omb_ref/omb_i)^5          18 n_c . normal     19 1/D_c^2
+  // The records are double-buffered (sub-tile k in sm[k & 1]), so one barrier per sub-tile suffices.
   constexpr int kPdFields = 20;
-  __shared__ float4 sm[kPdFields / 2][kSub / 2];
-  float *rec = &sm[0][0].x;
-  auto put = [&](int t, int f, float v) { rec[((f >> 1) * (kSub / 2) + (t >> 1)) * 4 + (f & 1) * 2 + (t & 1)] = v; };
+  __shared__ float4 sm[2][kPdFields / 2][kSub / 2];
   const int tid = threadIdx.x;
-  const int nt2 = (g.n2 + kTileB - 1) / kTileB;
-  const int T1 = blockIdx.x / nt2, T2 = blockIdx.x % nt2;
-  const int a = tid / kTileB, b = tid % kTileB;
-  const int i1 = T1 * kTileA + a, i2 = T2 * kTileB + b;
-  const bool active = i1 < g.n1 && i2 < g.n2;
-  const int64_t j = (int64_t)i1 * g.n2 + i2;
-  const int64_t np = (int64_t)g.n1 * g.n2;
+  const TilePoint P = strip_point(m, blockIdx.x, tid);
+  const bool active = P.active;
   const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
   const int64_t off = (int64_t)p * 3 * n;
   const double *xp = X + off, *bp = Bt + off, *ap = Ac + off;
   const int64_t i0 = (int64_t)s * chunk, iend = imin64(n, i0 + chunk);
-  const int ca = T1 * kTileA + kTileA / 2, cb = T2 * kTileB + kTileB / 2;
-  double Oc[3];
-  for (int c = 0; c < 3; ++c) Oc[c] = g.origin[c] + (double)ca * g.u1[c] + (double)cb * g.u2[c];
-  const int da = i1 - ca, db = i2 - cb;
-  float Dl[3];
-  for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);
-  const float2 Dx = f2(Dl[0], Dl[0]), Dy = f2(Dl[1], Dl[1]), Dz = f2(Dl[2], Dl[2]);
-  const float ddv = Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2];
-  const float2 dd = f2(ddv, ddv), one = f2(1.0f, 1.0f);
-  const float2 NRx = f2((float)nx_, (float)nx_), NRy = f2((float)ny_, (float)ny_), NRz = f2((float)nz_, (float)nz_);
+  const int da = P.i1 - P.ca, db = P.i2 - P.cb;
   double omb_ref;
   {
     const double bx = bp[0], by = bp[n], bz = bp[2 * n];
     const double b2 = bx * bx + by * by + bz * bz;
     omb_ref = (1.0 - b2) / (1.0 + sqrt(b2));
   }
-  double sum = 0;
-  for (int64_t base = i0; base < iend; base += kSub) {
+
+  auto fill = [&](int buf, int64_t base) {
+    float *rec = &sm[buf][0][0].x;
+    auto put = [&](int t, int f, float v) { rec[((f >> 1) * (kSub / 2) + (t >> 1)) * 4 + (f & 1) * 2 + (t & 1)] = v; };
     const int cnt = (int)imin64(kSub, iend - base);
-    __syncthreads();
     if (tid < cnt) {
       const int64_t i = base + tid;
+      double Oc[3];
+      for (int c = 0; c < 3; ++c) Oc[c] = g.origin[c] + (double)P.ca * g.u1[c] + (double)P.cb * g.u2[c];
       const Anchor A = make_anchor(Oc, xp, bp, n, i);
       const double ax = ap[i], ay = ap[n + i], az = ap[2 * n + i];
       const double r = omb_ref / A.omb;
@@ -131,48 +121,65 @@ __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__r
       put(tid, 7, (float)(0.5 * A.invDc));
       put(tid, 8, (float)(A.bhat[0] * A.omb)); put(tid, 9, (float)(A.bhat[1] * A.omb));
       put(tid, 10, (float)(A.bhat[2] * A.omb));
-      put(tid, 11, (float)A.omb);
+      put(tid, 11, (float)(-A.omb));
       put(tid, 12, (float)ax); put(tid, 13, (float)ay); put(tid, 14, (float)az);
       put(tid, 15, (float)(0.5 * A.bmag / A.omb));
       put(tid, 16, (float)(A.bhat[0] * ax + A.bhat[1] * ay + A.bhat[2] * az));
       put(tid, 17, (float)(r * r * r * r * r));
       put(tid, 18, (float)(A.nc[0] * nx_ + A.nc[1] * ny_ + A.nc[2] * nz_));
+      put(tid, 19, (float)(A.invDc * A.invDc));
     } else if (tid == cnt && (cnt & 1)) {
       // the odd count's partner slot: zero 1/D_c and (omb_ref/omb)^5 make its term 0; omb = 1 keeps
       // 1 - n.beta finite
-      for (int f = 0; f < 19; ++f) put(tid, f, f == 11 ? 1.0f : 0.0f);
+      for (int f = 0; f < kPdFields; ++f) put(tid, f, f == 11 ? -1.0f : 0.0f);
     }
-    __syncthreads();
+  };
+
+  double sum = 0;
+  if (i0 < iend) fill(0, i0);
+  int buf = 0;
+  for (int64_t base = i0; base < iend; base += kSub, buf ^= 1) {
+    const int cnt = (int)imin64(kSub, iend - base);
+    __syncthreads();  // records of this sub-tile complete; every thread is done with the other buffer
+    if (base + kSub < iend) fill(buf ^ 1, base + kSub);
     if (!active) continue;
+    // this thread's offset from the anchor point (formed after the FP64 anchors, off their registers)
+    float Dl[3];
+    for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);
+    const float2 Dx = f2(Dl[0], Dl[0]), Dy = f2(Dl[1], Dl[1]), Dz = f2(Dl[2], Dl[2]);
+    const float2 Dxn = f2(-Dl[0], -Dl[0]), Dyn = f2(-Dl[1], -Dl[1]), Dzn = f2(-Dl[2], -Dl[2]);
+    const float ddv = -(Dl[0] * Dl[0] + Dl[1] * Dl[1] + Dl[2] * Dl[2]);
+    const float2 ddn = f2(ddv, ddv), one = f2(1.0f, 1.0f);
+    const float2 NRx = f2((float)nx_, (float)nx_), NRy = f2((float)ny_, (float)ny_), NRz = f2((float)nz_, (float)nz_);
+    const float4(*sr)[kSub / 2] = sm[buf];
     float2 acc = f2(0.f, 0.f);
     const int pairs = (cnt + 1) >> 1;
 #pragma unroll 2
     for (int q = 0; q < pairs; ++q) {
-      const float4 R0 = sm[0][q], R1 = sm[1][q], R2 = sm[2][q], R3 = sm[3][q], R4 = sm[4][q];
-      const float4 R5 = sm[5][q], R6 = sm[6][q], R7 = sm[7][q], R8 = sm[8][q], R9 = sm[9][q];
+      const float4 R0 = sr[0][q], R1 = sr[1][q], R2 = sr[2][q], R3 = sr[3][q], R4 = sr[4][q];
+      const float4 R5 = sr[5][q], R6 = sr[6][q], R7 = sr[7][q], R8 = sr[8][q], R9 = sr[9][q];
       const float2 ncx = f2(R0.x, R0.y), ncy = f2(R0.z, R0.w), ncz = f2(R1.x, R1.y), w = f2(R1.z, R1.w);
       const float2 dcx = f2(R2.x, R2.y), dcy = f2(R2.z, R2.w), dcz = f2(R3.x, R3.y), hinv = f2(R3.z, R3.w);
-      const float2 box = f2(R4.x, R4.y), boy = f2(R4.z, R4.w), boz = f2(R5.x, R5.y), omb = f2(R5.z, R5.w);
+      const float2 box = f2(R4.x, R4.y), boy = f2(R4.z, R4.w), boz = f2(R5.x, R5.y), ombn = f2(R5.z, R5.w);
       const float2 acx = f2(R6.x, R6.y), acy = f2(R6.z, R6.w), acz = f2(R7.x, R7.y), bfac = f2(R7.z, R7.w);
-      const float2 ba = f2(R8.x, R8.y), r5 = f2(R8.z, R8.w), ncn = f2(R9.x, R9.y);
-      const float2 gq = fma2(ncz, Dz, fma2(ncy, Dy, mul2(ncx, Dx)));  // n_c . Delta
-      const float2 h = fma2(neg2(gq), gq, dd);
-      const float2 del = fma2(h, hinv, gq);                          // D_j - D_c
-      const float2 t = mul2(del, w);
-      const float2 rinv = fma2(neg2(t), w, w);                       // 1/D_j
-      const float2 dnx = mul2(fma2(neg2(ncx), del, Dx), rinv);       // n_j - n_c
-      const float2 dny = mul2(fma2(neg2(ncy), del, Dy), rinv);
-      const float2 dnz = mul2(fma2(neg2(ncz), del, Dz), rinv);
+      const float2 ba = f2(R8.x, R8.y), r5 = f2(R8.z, R8.w), ncn = f2(R9.x, R9.y), w2 = f2(R9.z, R9.w);
+      const float2 gqn = fma2(ncz, Dzn, fma2(ncy, Dyn, mul2(ncx, Dxn)));  // -n_c . Delta
+      const float2 hn = fma2(gqn, gqn, ddn);                              // -(|Delta|^2 - g^2)
+      const float2 deln = fma2(hn, hinv, gqn);                            // D_c - D_j
+      const float2 rinv = fma2(deln, w2, w);                              // 1/D_j
+      const float2 dnx = mul2(fma2(ncx, deln, Dx), rinv);                 // n_j - n_c
+      const float2 dny = mul2(fma2(ncy, deln, Dy), rinv);
+      const float2 dnz = mul2(fma2(ncz, deln, Dz), rinv);
       const float2 nd = fma2(dnz, NRz, fma2(dny, NRy, fma2(dnx, NRx, ncn)));  // n_j . normal
       const float2 dx = add2(dcx, dnx), dy = add2(dcy, dny), dz = add2(dcz, dnz);  // n_j - bhat
       const float2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
-      const float2 opn = fma2(bfac, d2, one);                        // (1 - n.beta) / omb_i
-      const float2 opnb = mul2(omb, opn);                            // 1 - n.beta
+      const float2 opn = fma2(bfac, d2, one);                            // (1 - n.beta) / omb_i
+      const float2 opnbn = mul2(ombn, opn);                              // -(1 - n.beta)
       const float2 na = fma2(dz, acz, fma2(dy, acy, fma2(dx, acx, ba)));  // n . a
       // V = n x ((n - beta) x a) = (n - beta)(n.a) - a (1 - n.beta)
-      const float2 Vx = fma2(add2(dx, box), na, mul2(neg2(acx), opnb));
-      const float2 Vy = fma2(add2(dy, boy), na, mul2(neg2(acy), opnb));
-      const float2 Vz = fma2(add2(dz, boz), na, mul2(neg2(acz), opnb));
+      const float2 Vx = fma2(add2(dx, box), na, mul2(acx, opnbn));
+      const float2 Vy = fma2(add2(dy, boy), na, mul2(acy, opnbn));
+      const float2 Vz = fma2(add2(dz, boz), na, mul2(acz, opnbn));
       const float2 v2 = fma2(Vz, Vz, fma2(Vy, Vy, mul2(Vx, Vx)));
       const float2 o2 = mul2(opn, opn);
       const float2 o5 = mul2(mul2(o2, o2), opn);
@@ -187,7 +194,7 @@ __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__r
     sum += (double)acc.x + (double)acc.y;
   }
   const double r2 = 1.0 / (omb_ref * omb_ref);
-  if (active) partial[((int64_t)p * S + s) * np + j] = sum * (r2 * r2 / omb_ref);
+  if (active) partial[((int64_t)p * S + s) * ((int64_t)g.n1 * g.n2) + (int64_t)P.i1 * g.n2 + P.i2] = sum * (r2 * r2 / omb_ref);
 }
 
 // ---------------------------------------------------------------- power density at a list of points
@@ -300,8 +307,7 @@ __global__ void omega_kernel(const double *__restrict__ e, int64_t ne, double *_
 // ---------------------------------------------------------------- launchers
 
 static int flux_mixed_splits(int64_t n, const srs_grid2d &g, int nparticles) {
-  GridTiles t = tiles_of(g);
-  return splits_for((int64_t)t.t1 * t.t2 * nparticles, n, 256, wave_slots(flux_mixed_kernel));
+  return splits_for((int64_t)strip_tiles(g).tiles * nparticles, n, 256, wave_slots(flux_mixed_kernel));
 }
 
 size_t mixed_flux_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles) {
@@ -312,11 +318,11 @@ static cudaError_t mixed_flux_splits(const srs_traj_view &t, const srs_beam_cons
                                      double energy_ev, double *d_out, void *scratch, int S_max, cudaStream_t s) {
   const int64_t chunk = aligned_chunk(t.n, S_max);
   const int S = used_chunks(t.n, chunk);
-  GridTiles tl = tiles_of(g);
+  const StripTiles m = strip_tiles(g);
   const double omega = ev_to_omega(energy_ev);
   double *partial = static_cast<double *>(scratch);
-  dim3 grid((unsigned)(tl.t1 * tl.t2), S, t.nparticles);
-  flux_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt, g, omega, chunk, partial);
+  dim3 grid((unsigned)m.tiles, S, t.nparticles);
+  flux_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt, g, m, omega, chunk, partial);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return finish_flux_partials(partial, S, (int64_t)g.n1 * g.n2, t.nparticles, nullptr, omega, t.dt, flux_c0(b.charge),
@@ -416,21 +422,20 @@ extern "C" srs_status srs_flux_mixed_noalloc(srs_traj_view traj, srs_beam_consts
 namespace srs {
 
 size_t mixed_pd_scratch_bytes(int64_t n, const srs_grid2d &g, int nparticles) {
-  GridTiles tl = tiles_of(g);
   return sizeof(double) * (size_t)g.n1 * g.n2 * nparticles *
-         splits_for((int64_t)tl.t1 * tl.t2 * nparticles, n, 256, wave_slots(pd_mixed_kernel));
+         splits_for((int64_t)strip_tiles(g).tiles * nparticles, n, 256, wave_slots(pd_mixed_kernel));
 }
 
 cudaError_t mixed_power_density(const srs_traj_view &t, const srs_beam_consts &b, const srs_grid2d &g,
                                 int directional, double *d_out, void *scratch, cudaStream_t s) {
-  GridTiles tl = tiles_of(g);
+  const StripTiles m = strip_tiles(g);
   const int64_t chunk =
-      aligned_chunk(t.n, splits_for((int64_t)tl.t1 * tl.t2 * t.nparticles, t.n, 256, wave_slots(pd_mixed_kernel)));
+      aligned_chunk(t.n, splits_for((int64_t)m.tiles * t.nparticles, t.n, 256, wave_slots(pd_mixed_kernel)));
   const int S = used_chunks(t.n, chunk);
   double *partial = static_cast<double *>(scratch);
-  dim3 grid((unsigned)(tl.t1 * tl.t2), S, t.nparticles);
-  pd_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.aoc, t.n, g, g.normal[0], g.normal[1], g.normal[2], directional, chunk,
-                                            partial);
+  dim3 grid((unsigned)m.tiles, S, t.nparticles);
+  pd_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.aoc, t.n, g, m, g.normal[0], g.normal[1], g.normal[2],
+                                            directional, chunk, partial);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return finish_pd_partials(partial, S, (int64_t)g.n1 * g.n2, t.nparticles, pd_const(b.charge, b.current) * t.dt,
