@@ -89,23 +89,46 @@ __global__ void __launch_bounds__(kTile) flux_fp64_kernel(const double *__restri
 }
 
 
-__global__ void flux_fp64_reduce(const double *__restrict__ partial, int S, int64_t np, int nparticles,
-                                 const double *__restrict__ omegas, double omega0, double dt, double C0, double C2,
-                                 double *__restrict__ out, double *__restrict__ e6) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= np * nparticles) return;
-  const int64_t p = idx / np, j = idx % np;
-  double e[6] = {0, 0, 0, 0, 0, 0};
-  for (int s = 0; s < S; ++s) {
-    const double *o = partial + ((int64_t)p * S + s) * 6 * np + j;
+// Block of kRedPoints x 6 threads: thread (c, k) adds component c of point j = block * kRedPoints + k
+// over the S chunks in chunk order (eight chunks' loads in flight at a time; the adds stay in order),
+// then one thread per point applies the final scaling.
+constexpr int kRedPoints = 32;
+__global__ void __launch_bounds__(6 * kRedPoints) flux_fp64_reduce(const double *__restrict__ partial, int S,
+                                                                   int64_t np, int nparticles,
+                                                                   const double *__restrict__ omegas, double omega0,
+                                                                   double dt, double C0, double C2,
+                                                                   double *__restrict__ out, double *__restrict__ e6) {
+  __shared__ double se[kRedPoints][7];
+  const int k = threadIdx.x % kRedPoints, c = threadIdx.x / kRedPoints;
+  const int64_t idx = (int64_t)blockIdx.x * kRedPoints + k;
+  const bool valid = idx < np * nparticles;
+  if (valid) {
+    const int64_t p = idx / np, j = idx % np;
+    const double *o = partial + (int64_t)p * S * 6 * np + c * np + j;
+    const int64_t stride = 6 * np;
+    double e = 0;
+    int s = 0;
+    for (; s + 8 <= S; s += 8, o += 8 * stride) {
+      double v[8];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) e[c] += o[c * np];
+      for (int u = 0; u < 8; ++u) v[u] = o[u * stride];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) e += v[u];
+    }
+    for (; s < S; ++s, o += stride) e += *o;
+    se[k][c] = e;
   }
-  const double omega = omegas ? omegas[j] : omega0;
-  out[idx] = finish_flux(e, omega, dt, C0, C2);
-  if (e6) {
+  __syncthreads();
+  if (c == 0 && valid) {
+    double e[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) e6[6 * idx + c] = e[c];
+    for (int q = 0; q < 6; ++q) e[q] = se[k][q];
+    const double omega = omegas ? omegas[idx % np] : omega0;
+    out[idx] = finish_flux(e, omega, dt, C0, C2);
+    if (e6) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) e6[6 * idx + q] = e[q];
+    }
   }
 }
 
@@ -226,7 +249,16 @@ __global__ void pd_fp64_reduce(const double *__restrict__ partial, int S, int64_
   if (idx >= np * nparticles) return;
   const int64_t p = idx / np, j = idx % np;
   double sum = 0;
-  for (int s = 0; s < S; ++s) sum += partial[((int64_t)p * S + s) * np + j];
+  const double *o = partial + (int64_t)p * S * np + j;
+  int s = 0;
+  for (; s + 8 <= S; s += 8, o += 8 * np) {  // chunk order, eight chunks' loads in flight at a time
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = o[u * np];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) sum += v[u];
+  }
+  for (; s < S; ++s, o += np) sum += *o;
   sum *= cdt;
   sum /= 1e6;
   if (!directional && sum < 0) sum *= -1;
@@ -319,7 +351,7 @@ cudaError_t fp64_flux(const srs_traj_view &t, const srs_beam_consts &b, const do
   double *partial = static_cast<double *>(scratch);
   dim3 grid((unsigned)((np + kTile - 1) / kTile), S, t.nparticles);
   flux_fp64_kernel<<<grid, kTile, 0, s>>>(t.x, t.beta, t.n, t.dt, d_points, np, omega, chunk, partial);
-  flux_fp64_reduce<<<blocks_for(np * t.nparticles, 256), 256, 0, s>>>(partial, S, np, t.nparticles, nullptr, omega,
+  flux_fp64_reduce<<<blocks_for(np * t.nparticles, kRedPoints), 6 * kRedPoints, 0, s>>>(partial, S, np, t.nparticles, nullptr, omega,
                                                                       t.dt, flux_c0(b.charge),
                                                                       flux_c2(b.charge, b.current), d_out, nullptr);
   return cudaGetLastError();
@@ -341,7 +373,7 @@ cudaError_t fp64_spectrum(const srs_traj_view &t, const srs_beam_consts &b, cons
   spectrum_fp64_kernel<<<grid, kTile, 0, s>>>(t.x, t.beta, t.n, t.dt, v3(obs[0], obs[1], obs[2]), d_energies, ne,
                                               chunk, partial);
   omegas_kernel<<<blocks_for(ne, 256), 256, 0, s>>>(d_energies, ne, omegas);
-  flux_fp64_reduce<<<blocks_for(ne * t.nparticles, 256), 256, 0, s>>>(partial, S, ne, t.nparticles, omegas, 0.0,
+  flux_fp64_reduce<<<blocks_for(ne * t.nparticles, kRedPoints), 6 * kRedPoints, 0, s>>>(partial, S, ne, t.nparticles, omegas, 0.0,
                                                                       t.dt, flux_c0(b.charge),
                                                                       flux_c2(b.charge, b.current), d_out, d_e6);
   return cudaGetLastError();
@@ -378,14 +410,14 @@ cudaError_t total_power(const srs_traj_view &t, const srs_beam_consts &b, const 
 cudaError_t finish_flux_partials(const double *partial, int S, int64_t nout, int nparticles, const double *omegas,
                                  double omega0, double dt, double C0, double C2, double *out, cudaStream_t s,
                                  double *e6) {
-  flux_fp64_reduce<<<blocks_for(nout * nparticles, 256), 256, 0, s>>>(partial, S, nout, nparticles, omegas, omega0, dt,
+  flux_fp64_reduce<<<blocks_for(nout * nparticles, kRedPoints), 6 * kRedPoints, 0, s>>>(partial, S, nout, nparticles, omegas, omega0, dt,
                                                                      C0, C2, out, e6);
   return cudaGetLastError();
 }
 
 cudaError_t finish_pd_partials(const double *partial, int S, int64_t np, int nparticles, double cdt, int directional,
                                double *out, cudaStream_t s) {
-  pd_fp64_reduce<<<blocks_for(np * nparticles, 256), 256, 0, s>>>(partial, S, np, nparticles, cdt, directional, out);
+  pd_fp64_reduce<<<blocks_for(np * nparticles, 128), 128, 0, s>>>(partial, S, np, nparticles, cdt, directional, out);
   return cudaGetLastError();
 }
 
