@@ -579,9 +579,10 @@ def run_ours(args, world, rank, local):
     o.set_trajectory_mode("auto")
     e2e_s = timed_e2e(e2e_steps)
     e2e = {"value": world * EVALS_PER_STEP * e2e_steps / e2e_s, "unit": UNIT,
-           # per map: accumulator and compensation arrays in, particle in (RK4 once per step); out: both arrays
-           "h2d_bytes_per_step": len(ENERGIES) * 2 * npts * 8 + 56,
-           "d2h_bytes_per_step": len(ENERGIES) * 2 * npts * 8,
+           # in: the particle (RK4 once per step; each map's sums start from zero on the device);
+           # out: each map's values
+           "h2d_bytes_per_step": 56,
+           "d2h_bytes_per_step": len(ENERGIES) * npts * 8,
            "ms_per_step": 1e3 * e2e_s / e2e_steps,
            "includes": "RK4 trajectory on the GPU (once per step, parallel in time), both maps, host<->device "
                        "copies of each call",

@@ -443,8 +443,9 @@ srs_status srs_sim_calculate_trajectory(srs_sim *sim, int64_t *n, double *x, dou
 
 /* The sums for the current particle (nparticles == 0) or nparticles sampled particles with weight
  * 1/nparticles; results are Kahan-added into out/comp (HOST, length nout), as the reference's
- * containers.  For the power density, weighted != 0 applies the weight (the reference's GPU path)
- * and 0 does not (its CPU paths). */
+ * containers.  comp == NULL: the sums start from zero and are written to out (its contents are not
+ * read), and the compensation stays on the device.  For the power density, weighted != 0 applies the
+ * weight (the reference's GPU path) and 0 does not (its CPU paths). */
 srs_status srs_sim_calculate_spectrum(srs_sim *sim, const double obs[3], const double *energies,
                                       int64_t ne, int32_t nparticles, int32_t precision, double *out,
                                       double *comp);

@@ -441,12 +441,17 @@ struct srs_sim {
       pinned_doubles = 2 * nout;
     }
     // the caller's accumulators go up after the first batch's sums are queued: the host copies them
-    // into pinned memory while the GPU computes
+    // into pinned memory while the GPU computes.  Without comp the sums start from zero on the device.
+    const bool fresh = comp == nullptr;
     bool uploaded = false;
     auto upload = [&]() -> srs_status {
-      std::memcpy(pinned, out, sizeof(double) * nout);
-      std::memcpy(pinned + nout, comp, sizeof(double) * nout);
-      SRS_CUDA(cudaMemcpyAsync(d_out, pinned, sizeof(double) * 2 * nout, cudaMemcpyHostToDevice, stream));
+      if (fresh) {
+        SRS_CUDA(cudaMemsetAsync(d_out, 0, sizeof(double) * 2 * nout, stream));
+      } else {
+        std::memcpy(pinned, out, sizeof(double) * nout);
+        std::memcpy(pinned + nout, comp, sizeof(double) * nout);
+        SRS_CUDA(cudaMemcpyAsync(d_out, pinned, sizeof(double) * 2 * nout, cudaMemcpyHostToDevice, stream));
+      }
       uploaded = true;
       return SRS_OK;
     };
@@ -475,10 +480,10 @@ struct srs_sim {
     }
     if (!uploaded)
       if (srs_status st = upload()) return st;
-    SRS_CUDA(cudaMemcpyAsync(pinned, d_out, sizeof(double) * 2 * nout, cudaMemcpyDeviceToHost, stream));
+    SRS_CUDA(cudaMemcpyAsync(pinned, d_out, sizeof(double) * (fresh ? 1 : 2) * nout, cudaMemcpyDeviceToHost, stream));
     SRS_CUDA(cudaStreamSynchronize(stream));
     std::memcpy(out, pinned, sizeof(double) * nout);
-    std::memcpy(comp, pinned + nout, sizeof(double) * nout);
+    if (!fresh) std::memcpy(comp, pinned + nout, sizeof(double) * nout);
     return SRS_OK;
   }
 };
@@ -952,7 +957,7 @@ srs_status srs_sim_calculate_trajectory(srs_sim *sim, int64_t *n, double *x, dou
 srs_status srs_sim_calculate_spectrum(srs_sim *sim, const double obs[3], const double *energies, int64_t ne,
                                       int32_t nparticles, int32_t precision, double *out, double *comp) {
   SIM_GUARD(sim);
-  if (!obs || !energies || !out || !comp || ne < 1) return fail(SRS_ERR_INVALID, "bad argument");
+  if (!obs || !energies || !out || ne < 1) return fail(SRS_ERR_INVALID, "bad argument");
   if (nparticles < 0) return fail(SRS_ERR_INVALID, "'nparticles' must be >= 1 (sort of)");
   DeviceBuffer de;
   SRS_CUDA(de.alloc(sizeof(double) * ne, sim->stream));
@@ -968,7 +973,7 @@ srs_status srs_sim_calculate_spectrum(srs_sim *sim, const double obs[3], const d
 srs_status srs_sim_calculate_flux(srs_sim *sim, const double *points, int64_t np, const srs_grid2d *grid,
                                   double energy_ev, int32_t nparticles, int32_t precision, double *out, double *comp) {
   SIM_GUARD(sim);
-  if (!out || !comp || np < 1 || (!points && !grid)) return fail(SRS_ERR_INVALID, "bad argument");
+  if (!out || np < 1 || (!points && !grid)) return fail(SRS_ERR_INVALID, "bad argument");
   if (nparticles < 0) return fail(SRS_ERR_INVALID, "'nparticles' must be >= 1 (sort of)");
   DeviceBuffer dp;
   const double *d_p = nullptr;
@@ -988,7 +993,7 @@ srs_status srs_sim_calculate_power_density(srs_sim *sim, const double *points, c
                                            const srs_grid2d *grid, int32_t directional, int32_t nparticles,
                                            int32_t weighted, int32_t precision, double *out, double *comp) {
   SIM_GUARD(sim);
-  if (!points || !normals || !out || !comp || np < 1) return fail(SRS_ERR_INVALID, "bad argument");
+  if (!points || !normals || !out || np < 1) return fail(SRS_ERR_INVALID, "bad argument");
   if (nparticles < 0) return fail(SRS_ERR_INVALID, "'nparticles' must be >= 1 (sort of)");
   DeviceBuffer dp;
   const double *d_p = nullptr, *d_n = nullptr;

@@ -428,9 +428,9 @@ class sr:  # noqa: N801  (the reference's type name)
             check(lib.srs_energy_grid(int(npoints), float(energy_range_eV[0]), float(energy_range_eV[1]), dptr(e)))
         else:
             e = np.ascontiguousarray(np.array(pts, dtype=np.float64))
-        out, comp = np.zeros(len(e)), np.zeros(len(e))
+        out = np.zeros(len(e))
         check(lib.srs_sim_calculate_spectrum(self._h, v3(o), dptr(e), len(e), int(nparticles), prec, dptr(out),
-                                             dptr(comp)))
+                                             None))
         return e, out
 
     # ------------------------------------------------------------ surfaces
@@ -549,11 +549,11 @@ class sr:  # noqa: N801  (the reference's type name)
             raise ValueError("'nparticles' must be >= 1 (sort of)")
         self._check_gpu_threads(gpu, nthreads)
         npts = len(xyz)
-        out, comp = np.zeros(npts), np.zeros(npts)
+        out = np.zeros(npts)
         if npts:
             pts = np.ascontiguousarray(xyz.reshape(-1))
             check(lib.srs_sim_calculate_flux(self._h, dptr(pts), npts, None, float(energy_eV), int(nparticles),
-                                             self._prec(precision), dptr(out), dptr(comp)))
+                                             self._prec(precision), dptr(out), None))
         C_, V = self._point_list(xyz, out, nparticles, nthreads, gpu, pd=False)
         if ofile:
             self._write_points(ofile, C_, V, 3)
@@ -571,13 +571,13 @@ class sr:  # noqa: N801  (the reference's type name)
             raise ValueError("'nparticles' must be >= 1 (sort of)")
         self._check_gpu_threads(gpu, nthreads)
         npts = len(xyz)
-        out, comp = np.zeros(npts), np.zeros(npts)
+        out = np.zeros(npts)
         if npts:
             pts = np.ascontiguousarray(xyz.reshape(-1))
             nrms = np.ascontiguousarray(nrm.reshape(-1))
             check(lib.srs_sim_calculate_power_density(self._h, dptr(pts), dptr(nrms), npts, None,
                                                       0 if normal == 0 else 1, int(nparticles), 1 if gpu == 1 else 0,
-                                                      self._prec(precision), dptr(out), dptr(comp)))
+                                                      self._prec(precision), dptr(out), None))
         C_, V = self._point_list(xyz, out, nparticles, nthreads, gpu, pd=True)
         if ofile:
             self._write_points(ofile, C_, V, 3)
@@ -603,10 +603,10 @@ class sr:  # noqa: N801  (the reference's type name)
         self._check_gpu_threads(gpu, nthreads)
         prec = self._prec(precision)
         npts = len(xyz)
-        out, comp = np.zeros(npts), np.zeros(npts)
+        out = np.zeros(npts)
         pts = np.ascontiguousarray(xyz.reshape(-1))
         check(lib.srs_sim_calculate_flux(self._h, dptr(pts), npts, C.byref(grid), float(energy_eV),
-                                         int(nparticles), prec, dptr(out), dptr(comp)))
+                                         int(nparticles), prec, dptr(out), None))
         nth = nthreads if nthreads >= 1 else self._nthreads_global
         calls = max(1, int(nparticles))
         coords = [self._coords(xyz, x12, dim)]
@@ -628,10 +628,10 @@ class sr:  # noqa: N801  (the reference's type name)
         """The flux on a rectangle as numpy arrays (points (N,3), values (N,)), without list building."""
         xyz, x12, nrm, grid = self._rectangle(npoints, plane, width, x0x1x2, rotations, translation, normal)
         npts = len(xyz)
-        out, comp = np.zeros(npts), np.zeros(npts)
+        out = np.zeros(npts)
         pts = np.ascontiguousarray(xyz.reshape(-1))
         check(lib.srs_sim_calculate_flux(self._h, dptr(pts), npts, C.byref(grid), float(energy_eV),
-                                         int(nparticles), self._prec(precision), dptr(out), dptr(comp)))
+                                         int(nparticles), self._prec(precision), dptr(out), None))
         return xyz, out
 
     # ------------------------------------------------------------ power density
@@ -656,12 +656,12 @@ class sr:  # noqa: N801  (the reference's type name)
         prec = self._prec(precision)
         directional = 0 if normal == 0 else 1
         npts = len(xyz)
-        out, comp = np.zeros(npts), np.zeros(npts)
+        out = np.zeros(npts)
         pts = np.ascontiguousarray(xyz.reshape(-1))
         nrms = np.ascontiguousarray(np.tile(nrm, npts))
         check(lib.srs_sim_calculate_power_density(self._h, dptr(pts), dptr(nrms), npts, C.byref(grid), directional,
                                                   int(nparticles), 1 if gpu == 1 else 0, prec, dptr(out),
-                                                  dptr(comp)))
+                                                  None))
         nth = nthreads if nthreads >= 1 else self._nthreads_global
         calls = max(1, int(nparticles))
         coords = [self._coords(xyz, x12, dim)]
@@ -683,12 +683,12 @@ class sr:  # noqa: N801  (the reference's type name)
         """Power density on a rectangle as numpy arrays (points (N,3), W/mm^2 (N,))."""
         xyz, x12, nrm, grid = self._rectangle(npoints, plane, width, x0x1x2, rotations, translation, normal)
         npts = len(xyz)
-        out, comp = np.zeros(npts), np.zeros(npts)
+        out = np.zeros(npts)
         pts = np.ascontiguousarray(xyz.reshape(-1))
         nrms = np.ascontiguousarray(np.tile(nrm, npts))
         check(lib.srs_sim_calculate_power_density(self._h, dptr(pts), dptr(nrms), npts, C.byref(grid),
                                                   0 if normal == 0 else 1, int(nparticles), int(bool(weighted)),
-                                                  self._prec(precision), dptr(out), dptr(comp)))
+                                                  self._prec(precision), dptr(out), None))
         return xyz, out
 
     # ------------------------------------------------------------ total power

@@ -366,6 +366,36 @@ def test_c_abi_rejects_bad_arguments():
                                      _vp(t), None))
 
 
+def test_sim_sums_fresh_and_accumulated_outputs():
+    """srs_sim_calculate_*: with comp the sums are Kahan-added into the caller's out/comp; without it
+    they start from zero on the device and overwrite out.  Both give the same first result, bit for bit,
+    and a second call with comp adds to the first."""
+    from srsoriginal_b200 import _lib
+    from srsoriginal_b200.sr import rectangle_points
+    o = new_sr(2001)
+    xyz, _, _, grid = rectangle_points([9, 7], "XY", [0.01, 0.01], translation=[0, 0, 30])
+    pts = np.ascontiguousarray(xyz.reshape(-1))
+    n = len(xyz)
+    for prec in (_lib.FP64, _lib.MIXED):
+        fresh = np.full(n, 123.0)  # not read without comp
+        _lib.check(_lib.lib.srs_sim_calculate_flux(o._h, _lib.dptr(pts), n, C.byref(grid), 150.0, 0, prec,
+                                                   _lib.dptr(fresh), None))
+        acc, comp = np.zeros(n), np.zeros(n)
+        for _ in range(2):
+            _lib.check(_lib.lib.srs_sim_calculate_flux(o._h, _lib.dptr(pts), n, C.byref(grid), 150.0, 0, prec,
+                                                       _lib.dptr(acc), _lib.dptr(comp)))
+        assert np.all(fresh > 0)
+        assert np.array_equal(acc, fresh + fresh)  # x + x is exact, and its compensation is 0
+        assert np.all(comp == 0)
+    e, obs = np.linspace(100.0, 300.0, 17), np.array([0.0, 0.0, 30.0])
+    s1, s2, c2 = np.full(len(e), -1.0), np.zeros(len(e)), np.zeros(len(e))
+    _lib.check(_lib.lib.srs_sim_calculate_spectrum(o._h, _lib.dptr(obs), _lib.dptr(e), len(e), 0, _lib.FP64,
+                                                   _lib.dptr(s1), None))
+    _lib.check(_lib.lib.srs_sim_calculate_spectrum(o._h, _lib.dptr(obs), _lib.dptr(e), len(e), 0, _lib.FP64,
+                                                   _lib.dptr(s2), _lib.dptr(c2)))
+    assert np.array_equal(s1, s2)
+
+
 def test_edge_cases_small_sizes():
     o = new_sr(2)  # two trajectory points
     s = o.calculate_spectrum(obs=[0, 0, 30], npoints=1, energy_range_eV=[150, 150])
