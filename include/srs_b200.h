@@ -452,6 +452,15 @@ srs_status srs_sim_calculate_spectrum(srs_sim *sim, const double obs[3], const d
 srs_status srs_sim_calculate_flux(srs_sim *sim, const double *points, int64_t np,
                                   const srs_grid2d *grid, double energy_ev, int32_t nparticles,
                                   int32_t precision, double *out, double *comp);
+/* The flux on a rectangle given as srs_rectangle_plane takes it (calculate_flux_rectangle with
+ * plane and width, OSCARSSR_Python.cc:3009-3233), in one call: out, comp as srs_sim_calculate_flux;
+ * xyz (3*n1*n2), x12 (2*n1*n2) and nrm receive the surface (each may be NULL).  With
+ * SRS_PRECISION_MIXED the sums walk the grid and the points are written while the GPU computes;
+ * otherwise they are built first and uploaded.  rotations / translation NULL: zero. */
+srs_status srs_sim_calculate_flux_plane(srs_sim *sim, const char *plane, int32_t n1, int32_t n2, double w1,
+                                        double w2, const double rotations[3], const double translation[3],
+                                        int32_t normal, double energy_ev, int32_t nparticles, int32_t precision,
+                                        double *out, double *comp, double *xyz, double *x12, double nrm[3]);
 srs_status srs_sim_calculate_power_density(srs_sim *sim, const double *points, const double *normals,
                                            int64_t np, const srs_grid2d *grid, int32_t directional,
                                            int32_t nparticles, int32_t weighted, int32_t precision,

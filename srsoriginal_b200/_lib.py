@@ -135,6 +135,8 @@ def _load():
         "srs_sim_calculate_spectrum": (S, [P, _D, _D, C.c_int64, C.c_int32, C.c_int32, _D, _D]),
         "srs_sim_calculate_flux": (S, [P, _D, C.c_int64, C.POINTER(Grid2D), C.c_double, C.c_int32,
                                        C.c_int32, _D, _D]),
+        "srs_sim_calculate_flux_plane": (S, [P, C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_double, _D, _D,
+                                             C.c_int32, C.c_double, C.c_int32, C.c_int32, _D, _D, _D, _D, _D]),
         "srs_sim_calculate_power_density": (S, [P, _D, _D, C.c_int64, C.POINTER(Grid2D), C.c_int32,
                                                 C.c_int32, C.c_int32, C.c_int32, _D, _D]),
         "srs_sim_calculate_total_power": (S, [P, _D]),
@@ -179,7 +181,7 @@ EXPORTED = (
     "srs_sim_get_bfield srs_sim_set_field_grid_data srs_sim_add_particle_beam "
     "srs_sim_clear_particle_beams srs_sim_get_nparticle_beams srs_sim_set_new_particle "
     "srs_sim_get_particle srs_set_seed srs_random_uniform srs_random_normal srs_random_reset "
-    "srs_sim_calculate_trajectory srs_sim_calculate_spectrum srs_sim_calculate_flux "
+    "srs_sim_calculate_trajectory srs_sim_calculate_spectrum srs_sim_calculate_flux srs_sim_calculate_flux_plane "
     "srs_sim_calculate_power_density srs_sim_calculate_total_power srs_energy_grid "
     "srs_rectangle_plane srs_rectangle_points srs_measure_peak srs_flux_mixed_noalloc "
     "srs_queue_create srs_queue_run srs_queue_info srs_queue_destroy srs_trajectory_batch "

@@ -11,6 +11,7 @@
 #include <cctype>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <fstream>
 #include <map>
 #include <memory>
@@ -423,9 +424,11 @@ struct srs_sim {
 
   // The common driver: sample particles, integrate in batches, run `sum` on each batch (writing
   // per-particle values to d_vals), then Kahan-accumulate them in particle order into out/comp.
+  // host_work, when given, runs after all device work of the call is queued and before the host
+  // waits for it (host-side preparation of the call's other outputs, overlapped with the GPU)
   template <class SumFn>
   srs_status run(int32_t nparticles, int64_t nout, double *out, double *comp, bool apply_weight, int32_t precision,
-                 SumFn sum) {
+                 SumFn sum, const std::function<void()> &host_work = {}) {
     std::vector<Particle> ps;
     double weight;
     if (srs_status st = particles_for(nparticles, ps, weight)) return st;
@@ -481,6 +484,7 @@ struct srs_sim {
     if (!uploaded)
       if (srs_status st = upload()) return st;
     SRS_CUDA(cudaMemcpyAsync(pinned, d_out, sizeof(double) * (fresh ? 1 : 2) * nout, cudaMemcpyDeviceToHost, stream));
+    if (host_work) host_work();
     SRS_CUDA(cudaStreamSynchronize(stream));
     std::memcpy(out, pinned, sizeof(double) * nout);
     if (!fresh) std::memcpy(comp, pinned + nout, sizeof(double) * nout);
@@ -987,6 +991,54 @@ srs_status srs_sim_calculate_flux(srs_sim *sim, const double *points, int64_t np
                   [&](const srs_traj_view &v, const srs_beam_consts &bc, double *dv) {
     return srs_flux(v, bc, d_p, np, grid, energy_ev, precision, dv, s);
   });
+}
+
+srs_status srs_sim_calculate_flux_plane(srs_sim *sim, const char *plane, int32_t n1, int32_t n2, double w1,
+                                        double w2, const double rotations[3], const double translation[3],
+                                        int32_t normal, double energy_ev, int32_t nparticles, int32_t precision,
+                                        double *out, double *comp, double *xyz, double *x12, double nrm[3]) {
+  SIM_GUARD(sim);
+  if (!out) return fail(SRS_ERR_INVALID, "bad argument");
+  if (nparticles < 0) return fail(SRS_ERR_INVALID, "'nparticles' must be >= 1 (sort of)");
+  const double zero[3] = {0, 0, 0};
+  if (!rotations) rotations = zero;
+  if (!translation) translation = zero;
+  srs_grid2d grid;
+  double nv[3];
+  if (srs_status st = srs_rectangle_plane(plane, n1, n2, w1, w2, rotations, translation, normal, nullptr, nullptr,
+                                          nv, &grid))
+    return st;
+  if (nrm) std::memcpy(nrm, nv, sizeof nv);
+  const int64_t np = (int64_t)n1 * n2;
+  // the points: built while the GPU computes when the mixed kernel walks the grid, else first (uploaded)
+  auto emit = [&](double *p, double *q) {
+    srs_rectangle_plane(plane, n1, n2, w1, w2, rotations, translation, normal, p, q, nullptr, nullptr);
+  };
+  const bool walk = precision == SRS_PRECISION_MIXED;
+  DeviceBuffer dp;
+  const double *d_p = nullptr;
+  std::vector<double> tmp;
+  if (!walk) {
+    double *p = xyz;
+    if (!p) {
+      tmp.resize((size_t)(3 * np));
+      p = tmp.data();
+    }
+    emit(p, x12);
+    SRS_CUDA(dp.alloc(sizeof(double) * 3 * np, sim->stream));
+    SRS_CUDA(cudaMemcpyAsync(dp.ptr, p, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, sim->stream));
+    d_p = dp.as<double>();
+  }
+  cudaStream_t s = sim->stream;
+  const std::function<void()> host_work = [&]() {
+    if (walk && (xyz || x12)) emit(xyz, x12);
+  };
+  return sim->run(
+      nparticles, np, out, comp, true, precision,
+      [&](const srs_traj_view &v, const srs_beam_consts &bc, double *dv) {
+        return srs_flux(v, bc, d_p, np, &grid, energy_ev, precision, dv, s);
+      },
+      host_work);
 }
 
 srs_status srs_sim_calculate_power_density(srs_sim *sim, const double *points, const double *normals, int64_t np,

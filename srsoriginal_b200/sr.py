@@ -434,7 +434,8 @@ class sr:  # noqa: N801  (the reference's type name)
         return e, out
 
     # ------------------------------------------------------------ surfaces
-    def _rectangle(self, npoints, plane, width, x0x1x2, rotations, translation, normal):
+    @staticmethod
+    def _rect_spec(npoints, width, rotations, translation):
         if not isinstance(npoints, (list, tuple)) or len(npoints) != 2:
             raise ValueError("'npoints' must be [int, int]")
         n1, n2 = int(npoints[0]), int(npoints[1])
@@ -445,6 +446,10 @@ class sr:  # noqa: N801  (the reference's type name)
         w1 = w2 = 0.0
         if width is not None and len(width) == 2:
             w1, w2 = float(width[0]), float(width[1])
+        return n1, n2, w1, w2, rot, tr
+
+    def _rectangle(self, npoints, plane, width, x0x1x2, rotations, translation, normal):
+        n1, n2, w1, w2, rot, tr = sr._rect_spec(npoints, width, rotations, translation)
         np_ = n1 * n2
         xyz, x12 = np.zeros(3 * np_), np.zeros(2 * np_)
         nrm = _lib._V3()
@@ -625,7 +630,19 @@ class sr:  # noqa: N801  (the reference's type name)
 
     def flux_arrays(self, energy_eV, npoints, plane="", width=None, rotations=None, translation=None, x0x1x2=None,
                     nparticles=0, precision=None, normal=0):
-        """The flux on a rectangle as numpy arrays (points (N,3), values (N,)), without list building."""
+        """The flux on a rectangle as numpy arrays (points (N,3), values (N,)), without list building.
+        A plane and width (and no x0x1x2) go to the device in one call that builds the points while
+        the GPU computes."""
+        if plane and (x0x1x2 is None or len(x0x1x2) == 0):
+            n1, n2, w1, w2, rot, tr = sr._rect_spec(npoints, width, rotations, translation)
+            if w1 > 0 and w2 > 0:
+                npts = n1 * n2
+                xyz, out = np.empty(3 * npts), np.zeros(npts)
+                check(lib.srs_sim_calculate_flux_plane(self._h, str(plane).encode(), n1, n2, w1, w2, v3(rot), v3(tr),
+                                                       int(normal), float(energy_eV), int(nparticles),
+                                                       self._prec(precision), dptr(out), None, dptr(xyz), None,
+                                                       None))
+                return xyz.reshape(npts, 3), out
         xyz, x12, nrm, grid = self._rectangle(npoints, plane, width, x0x1x2, rotations, translation, normal)
         npts = len(xyz)
         out = np.zeros(npts)

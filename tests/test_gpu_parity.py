@@ -396,6 +396,38 @@ def test_sim_sums_fresh_and_accumulated_outputs():
     assert np.array_equal(s1, s2)
 
 
+def test_flux_plane_one_call_matches_points_call():
+    """srs_sim_calculate_flux_plane (rectangle built on the host while the GPU computes) gives the same
+    surface and the same values, bit for bit, as building the rectangle first and calling
+    srs_sim_calculate_flux with its points and grid."""
+    from srsoriginal_b200 import _lib
+    from srsoriginal_b200.sr import rectangle_points
+    o = new_sr(2001)
+    for plane, npts, rot, prec in (("XY", [9, 7], [0, 0, 0], _lib.MIXED), ("ZY", [6, 11], [0.1, -0.2, 0.3], _lib.MIXED),
+                                   ("XY", [9, 7], [0, 0, 0], _lib.FP64), ("YX", [5, 4], [0, 0.2, 0], _lib.FP64)):
+        xyz0, x120, nrm0, grid = rectangle_points(npts, plane, [0.01, 0.008], rotations=rot,
+                                                  translation=[0.001, 0, 30])
+        n = len(xyz0)
+        pts = np.ascontiguousarray(xyz0.reshape(-1))
+        ref = np.zeros(n)
+        _lib.check(_lib.lib.srs_sim_calculate_flux(o._h, _lib.dptr(pts), n, C.byref(grid), 150.0, 0, prec,
+                                                   _lib.dptr(ref), None))
+        out, xyz, x12, nrm = np.zeros(n), np.empty(3 * n), np.empty(2 * n), np.empty(3)
+        _lib.check(_lib.lib.srs_sim_calculate_flux_plane(o._h, plane.encode(), npts[0], npts[1], 0.01, 0.008,
+                                                         _lib.v3(rot), _lib.v3([0.001, 0, 30]), 0, 150.0, 0, prec,
+                                                         _lib.dptr(out), None, _lib.dptr(xyz), _lib.dptr(x12),
+                                                         _lib.dptr(nrm)))
+        assert np.array_equal(out, ref)
+        assert np.array_equal(xyz, xyz0.reshape(-1)) and np.array_equal(x12, x120.reshape(-1))
+        assert np.array_equal(nrm, nrm0)
+        p2, v2 = o.flux_arrays(150.0, npts, plane, [0.01, 0.008], rotations=rot, translation=[0.001, 0, 30],
+                               precision="mixed" if prec == _lib.MIXED else "fp64")
+        assert np.array_equal(v2, ref) and np.array_equal(p2, xyz0)
+    with pytest.raises(ValueError, match="surface string"):
+        _lib.check(_lib.lib.srs_sim_calculate_flux_plane(o._h, b"QQ", 3, 3, 0.01, 0.01, None, None, 0, 150.0, 0,
+                                                         _lib.MIXED, _lib.dptr(np.zeros(9)), None, None, None, None))
+
+
 def test_edge_cases_small_sizes():
     o = new_sr(2)  # two trajectory points
     s = o.calculate_spectrum(obs=[0, 0, 30], npoints=1, energy_range_eV=[150, 150])
@@ -519,4 +551,31 @@ def test_mixed_point_list_kernels_match_grid_kernels():
     D.power_density(t2, -O.QE, 0.5, a, points=pts, normals=nrms, precision=_lib.MIXED)
     D.power_density(t2, -O.QE, 0.5, c, points=pts, normals=nrms, precision=_lib.FP64)
     torch.cuda.synchronize()
+    assert_mixed(a.cpu().numpy(), c.cpu().numpy())
+
+
+@pytest.mark.parametrize("n1,n2", [(2, 17), (17, 2), (3, 5), (5, 200), (200, 5), (13, 13), (129, 7), (37, 101)])
+def test_mixed_grid_tiles_ragged_shapes(n1, n2):
+    """The grid mixed kernels tile the map into strips of 8-16 points (narrower strips for n2 < 8) and
+    take 128 consecutive points of a strip per CTA: every shape gives every point once, within the
+    mixed tolerance of the plain FP64 kernels on the same points."""
+    import torch
+    from srsoriginal_b200 import _lib, device as D
+    from srsoriginal_b200.sr import rectangle_points
+    tr = reference_trajectory_on_device(2001)
+    xyz, _, nrm, grid = rectangle_points([n1, n2], "XY", [0.004, 0.006], translation=[0, 0, 30])
+    n = n1 * n2
+    pts = torch.as_tensor(np.ascontiguousarray(xyz.reshape(-1)), device="cuda")
+    nrms = torch.as_tensor(np.ascontiguousarray(np.tile(nrm, (n, 1)).reshape(-1)), device="cuda")
+    a, c = (torch.full((n,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(2))
+    D.flux(tr, -O.QE, 0.5, W.E1_EV, a, grid=grid, precision=_lib.MIXED)
+    D.flux(tr, -O.QE, 0.5, W.E1_EV, c, points=pts, precision=_lib.FP64)
+    torch.cuda.synchronize()
+    assert np.all(np.isfinite(a.cpu().numpy()))
+    assert_mixed(a.cpu().numpy(), c.cpu().numpy())
+    a.fill_(float("nan"))
+    D.power_density(tr, -O.QE, 0.5, a, grid=grid, precision=_lib.MIXED)
+    D.power_density(tr, -O.QE, 0.5, c, points=pts, normals=nrms, precision=_lib.FP64)
+    torch.cuda.synchronize()
+    assert np.all(np.isfinite(a.cpu().numpy()))
     assert_mixed(a.cpu().numpy(), c.cpu().numpy())
