@@ -7,6 +7,9 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "srs_device.cuh"
 
@@ -48,13 +51,28 @@ inline int64_t aligned_chunk(int64_t n, int S) {
 }
 inline int used_chunks(int64_t n, int64_t chunk) { return (int)((n + chunk - 1) / chunk); }
 
-// Resident CTAs of `kernel` (kThreads threads, no dynamic shared memory) on the current device.
+// Resident CTAs of `kernel` (kThreads threads, no dynamic shared memory) on the current device,
+// queried once per (kernel, device): the launchers ask on every call.
 template <typename K>
 inline int64_t wave_slots(K kernel) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int64_t> cache;
   int dev = 0, sms = 148, occ = 1;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const bool have_dev = cudaGetDevice(&dev) == cudaSuccess;
+  const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), dev);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  if (have_dev) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kThreads, 0) != cudaSuccess || occ < 1) occ = 1;
-  return (int64_t)sms * occ;
+  const int64_t slots = (int64_t)sms * occ;
+  if (have_dev) {
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = slots;
+  }
+  return slots;
 }
 
 // Observation-grid tiles.  The u2 axis is cut into strips of balanced width (8 to 16 points when the
@@ -380,19 +398,20 @@ struct SpecShared {
   float v[10][kSub];
 };
 
-// Each thread owns kEnergiesPerThread consecutive energies.  The rotation exp(i dw tau_i) is shared by
+// Each thread owns K consecutive energies (kEnergiesPerThread, or 2 for spectra too small to fill
+// the GPU otherwise).  The rotation exp(i dw tau_i) is shared by
 // all threads (dw = (w_last - w_first)/(ne - 1), computed once per trajectory point per CTA); a thread
 // whose energies are not on that uniform grid (|w_k - (w_0 + k dw)| * tau_max > 1e-3 rad) takes one
 // reduced sincos per (point, energy) instead.  No host synchronisation is needed to decide.
-// One tile: energies of tile `etile` (kThreads * kEnergiesPerThread of them) against trajectory
-// points [i0, iend); writes the six partial sums of every energy to out6[c * ne + k].
+// One tile: energies of tile `etile` (kThreads * K of them, K per thread) against trajectory points
+// [i0, iend); writes the six partial sums of every energy to out6[c * ne + k].
+template <int K>
 __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, const double *__restrict__ bp,
                                               int64_t n, double dt, V3 obs, const double *__restrict__ omegas,
                                               int64_t ne, int etile, int64_t i0, int64_t iend,
                                               double *__restrict__ out6, SpecShared &sh) {
   double *stau = sh.tau;
   float (*sv)[kSub] = sh.v;  // a = (beta - n)/D (3), b' = n/D^2 (3), exp(i dw tau) (2), exp(2 i dw tau) (2)
-  constexpr int K = kEnergiesPerThread;
   const int tid = threadIdx.x;
   const int64_t k0 = ((int64_t)etile * kThreads + tid) * K;
   const bool active = k0 < ne;
@@ -440,9 +459,11 @@ __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, con
       sincos(reduce_2pi(dw * tau), &sr, &cr);
       sv[6][tid] = (float)cr;
       sv[7][tid] = (float)sr;
-      sincos(reduce_2pi(2.0 * dw * tau), &sr, &cr);  // the rotation by two energy steps
-      sv[8][tid] = (float)cr;
-      sv[9][tid] = (float)sr;
+      if (K > 2) {
+        sincos(reduce_2pi(2.0 * dw * tau), &sr, &cr);  // the rotation by two energy steps
+        sv[8][tid] = (float)cr;
+        sv[9][tid] = (float)sr;
+      }
     }
     __syncthreads();
     if (!active) continue;

@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(kThreads) queue_kernel(const QJob *__restrict_
     if (J.kind == SRS_JOB_FLUX)
       flux_tile(J.x, J.beta, J.n, J.dt, J.g, J.tiles, J.omega, w.tile, i0, i1, out6, sh.f);
     else
-      spectrum_tile(J.x, J.beta, J.n, J.dt, J.obs, J.omegas, J.ne, w.tile, i0, i1, out6, sh.s);
+      spectrum_tile<kEnergiesPerThread>(J.x, J.beta, J.n, J.dt, J.obs, J.omegas, J.ne, w.tile, i0, i1, out6, sh.s);
   }
 }
 

@@ -286,6 +286,7 @@ __global__ void __launch_bounds__(kThreads) pd_points_mixed_kernel(const double 
 
 // ---------------------------------------------------------------- spectrum at one observer
 
+template <int K>
 __global__ void __launch_bounds__(kThreads) spectrum_mixed_kernel(const double *__restrict__ X,
                                                                   const double *__restrict__ Bt, int64_t n, double dt,
                                                                   V3 obs, const double *__restrict__ omegas, int64_t ne,
@@ -293,8 +294,8 @@ __global__ void __launch_bounds__(kThreads) spectrum_mixed_kernel(const double *
   __shared__ tiles::SpecShared sh;
   const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
   const int64_t i0 = (int64_t)s * chunk;
-  tiles::spectrum_tile(X + (int64_t)p * 3 * n, Bt + (int64_t)p * 3 * n, n, dt, obs, omegas, ne, blockIdx.x, i0,
-                       imin64(n, i0 + chunk), partial + ((int64_t)p * S + s) * 6 * ne, sh);
+  tiles::spectrum_tile<K>(X + (int64_t)p * 3 * n, Bt + (int64_t)p * 3 * n, n, dt, obs, omegas, ne, blockIdx.x, i0,
+                          imin64(n, i0 + chunk), partial + ((int64_t)p * S + s) * 6 * ne, sh);
 }
 
 __global__ void omega_kernel(const double *__restrict__ e, int64_t ne, double *__restrict__ w) {
@@ -464,24 +465,56 @@ cudaError_t mixed_power_density_points(const srs_traj_view &t, const srs_beam_co
   return finish_pd_partials(partial, S, np, t.nparticles, pd_const(b.charge, b.current) * t.dt, directional, d_out, s);
 }
 
+// Energies per thread and trajectory chunks of a spectrum launch: kEnergiesPerThread with chunks of at
+// least two sub-tiles when those CTAs fill one wave; otherwise (one observer's spectrum of a few
+// thousand energies) two energies per thread and chunks down to one sub-tile, so that more CTAs share
+// the work, but at most 64 chunks (the reduction adds a point's chunks one after another).
+struct SpecPlan {
+  int K;
+  int64_t etiles;
+  int S_max;
+};
+static SpecPlan spectrum_plan(int64_t n, int64_t ne, int nparticles) {
+  constexpr int K4 = kEnergiesPerThread;
+  const int64_t slots4 = wave_slots(spectrum_mixed_kernel<K4>);
+  const int64_t e4 = (ne + kThreads * K4 - 1) / (kThreads * K4);
+  SpecPlan P;
+  if (e4 * nparticles * std::max<int64_t>(1, n / 256) >= slots4) {
+    P.K = K4;
+    P.etiles = e4;
+    P.S_max = splits_for(e4 * nparticles, n, 256, slots4);
+  } else {
+    P.K = 2;
+    P.etiles = (ne + kThreads * 2 - 1) / (kThreads * 2);
+    P.S_max = splits_for(P.etiles * nparticles, n, std::max<int64_t>(kSub, (n + 63) / 64),
+                         wave_slots(spectrum_mixed_kernel<2>));
+  }
+  return P;
+}
+
 size_t mixed_spectrum_scratch_bytes(int64_t n, int64_t ne, int nparticles) {
-  const int64_t ctas = (ne + kThreads * kEnergiesPerThread - 1) / (kThreads * kEnergiesPerThread) * nparticles;
-  return sizeof(double) * ((size_t)6 * ne * nparticles * splits_for(ctas, n, 256, wave_slots(spectrum_mixed_kernel)) + ne);
+  return sizeof(double) * ((size_t)6 * ne * nparticles * spectrum_plan(n, ne, nparticles).S_max + ne);
 }
 
 cudaError_t mixed_spectrum(const srs_traj_view &t, const srs_beam_consts &b, const double obs[3],
                            const double *d_energies, int64_t ne, double *d_out, void *scratch, cudaStream_t s,
                            double *d_e6) {
-  const int64_t etiles = (ne + kThreads * kEnergiesPerThread - 1) / (kThreads * kEnergiesPerThread);
-  const int S_max = splits_for(etiles * t.nparticles, t.n, 256, wave_slots(spectrum_mixed_kernel));
+  const SpecPlan plan = spectrum_plan(t.n, ne, t.nparticles);
+  const int64_t etiles = plan.etiles;
+  const int S_max = plan.S_max;
   const int64_t chunk = aligned_chunk(t.n, S_max);
   const int S = used_chunks(t.n, chunk);
   double *partial = static_cast<double *>(scratch);
   double *omegas = partial + (size_t)6 * ne * t.nparticles * S_max;  // after the S_max chunks sized for
   omega_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(d_energies, ne, omegas);
   dim3 grid((unsigned)etiles, S, t.nparticles);
-  spectrum_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt, v3(obs[0], obs[1], obs[2]), omegas, ne,
-                                                  chunk, partial);
+  if (plan.K == 2)
+    spectrum_mixed_kernel<2><<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt, v3(obs[0], obs[1], obs[2]), omegas,
+                                                       ne, chunk, partial);
+  else
+    spectrum_mixed_kernel<kEnergiesPerThread><<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt,
+                                                                        v3(obs[0], obs[1], obs[2]), omegas, ne,
+                                                                        chunk, partial);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return finish_flux_partials(partial, S, ne, t.nparticles, omegas, 0.0, t.dt, flux_c0(b.charge),

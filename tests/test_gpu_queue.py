@@ -57,7 +57,12 @@ def test_queue_matches_one_shot(small_specs):
         torch.cuda.synchronize()
         ref, ref64 = ref.cpu().numpy(), ref64.cpu().numpy()
         assert np.all(np.isfinite(got))
-        assert _rel(got, ref) <= 1e-12, s           # same sub-tile sums, other chunk grouping
+        if s["kind"] == "flux":
+            assert _rel(got, ref) <= 1e-12, s       # same sub-tile sums, other chunk grouping
+        else:
+            # a one-shot spectrum of a few thousand energies runs two energies per thread (the queue four):
+            # the rotation recurrence starts at other energies, the FP32 roundings differ
+            assert _rel(got, ref) <= 1e-6, s
         assert _rel(got, ref64) <= 1e-4, s          # mixed vs plain FP64
     # a second run of the captured graph gives the same numbers (deterministic reduction)
     first = [keep[-1].clone() for _, keep in jobs]
