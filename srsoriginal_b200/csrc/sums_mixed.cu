@@ -6,18 +6,20 @@
 // :1477-1598 power density), reorganised for the B200:
 //
 // * Flux / power density on a regular grid of observation points (a rectangle surface): a CTA owns
-//   an 8 x 16 tile of points and one chunk of the trajectory.  For each trajectory point i the CTA
-//   computes ONCE, in FP64, an anchor at the tile's centre point c: distance D_c, direction n_c, the
+//   a tile of up to 128 points (consecutive points of a strip 8-16 points wide, at most 17 rows) and
+//   one chunk of the trajectory.  For each trajectory point i the CTA computes ONCE, in FP64, an
+//   anchor at the tile's middle point c: distance D_c, direction n_c, the
 //   reduced phase Phi_c = w (t_i + D_c/c) mod 2pi, the reduced per-grid-step phase increments
 //   k1,k2 = (w/c) n_c.u1,u2 mod 2pi, and n_c - beta_hat.  Every point j = c + da*u1 + db*u2 of the
 //   tile then needs only FP32 work on small quantities:
 //       g = n_c . Delta_j,  h = |Delta_j|^2 - g^2,
-//       D_j - D_c = g + h/(2 D_c) (1 - g/D_c) + O(|Delta|^4/D^3),
-//       phase_j = Phi_c + k1 da + k2 db + (w/c) h/(2 D_c) (1 - g/D_c),
+//       D_j - D_c = g + h/(2 D_c) + O(g h/D_c^2)  (the dropped term is below FP32 resolution of the
+//                                                   phase for the tiles' extent at metres of distance),
+//       phase_j = Phi_c + k1 da + k2 db + (w/c) h/(2 D_c),
 //       n_j - beta_hat = (n_c - beta_hat) + (Delta_j - n_c (D_j - D_c)) / D_j,
 //   so no FP32 quantity is ever the difference of two nearly equal large numbers.
 //   1 - n.beta = (1 - |beta|) + |beta| |n - beta_hat|^2 / 2 (both terms >= 0, no cancellation).
-// * Spectrum on a uniform energy grid: a thread owns 4 consecutive energies; per trajectory point it
+// * Spectrum on a uniform energy grid: a thread owns 4 (or 2) consecutive energies; per trajectory point it
 //   forms one FP64 anchor exp(i w_k0 tau_i) and walks the others with the per-point rotation
 //   exp(i dw tau_i) (computed once per point per CTA in FP64), re-anchored at every point.  A
 //   non-uniform grid gets one reduced sincos per (point, energy).

@@ -3,7 +3,7 @@ persistent launch (srs_queue_*), replayed from a CUDA graph, with an autotuner f
 
 The reference runs such a set as separate calls (``calculate_spectrum`` / ``calculate_flux_rectangle``
 per job, OSCARSSR_Python.cc:2232 and :3033), each with its own launches and host synchronisation.  Here
-the jobs are cut into work items of one shape -- a tile of 8 x 16 grid points or 512 energies against
+the jobs are cut into work items of one shape -- a tile of up to 128 grid points or 512 energies against
 ``chunk`` trajectory points -- ordered longest first and drained by resident CTAs from an atomic
 ticket.  The tunable shape is (chunk, CTAs per SM); :func:`autotune` times the candidates on the jobs
 themselves and caches the winner per job-set signature and device in a JSON file.

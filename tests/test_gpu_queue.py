@@ -14,7 +14,7 @@ def _rel(a, b):
 
 @pytest.fixture(scope="module")
 def small_specs():
-    # mixed kinds and sizes, ragged edges on every axis (grid not a multiple of the 8 x 16 tile,
+    # mixed kinds and sizes, ragged edges on every axis (grids whose strips end in partial tiles,
     # energies not a multiple of 512, trajectory lengths not multiples of the chunk)
     return [dict(kind="flux", nt=5001, n=8), dict(kind="spectrum", nt=7003, ne=100),
             dict(kind="flux", nt=9001, n=37), dict(kind="spectrum", nt=5001, ne=1537),
