@@ -112,10 +112,11 @@ inline StripTiles strip_tiles(int n1, int n2) {
 }
 inline StripTiles strip_tiles(const srs_grid2d &g) { return strip_tiles(g.n1, g.n2); }
 
-// Thread tid's grid point (i1, i2) in tile `tile`, whether it holds one, and the tile's anchor point
-// (ca, cb): the middle row of the tile's points and the middle column of its strip.
+// Thread tid's grid point (i1, i2) in tile `tile`, whether it holds one, the tile's anchor point
+// (ca, cb): the middle row of the tile's points and the middle column of its strip, and the largest
+// |i1 - ca| and |i2 - cb| over the tile (ra, rb).
 struct TilePoint {
-  int i1, i2, ca, cb;
+  int i1, i2, ca, cb, ra, rb;
   bool active;
 };
 __host__ __device__ inline TilePoint strip_point(const StripTiles &m, int tile, int tid) {
@@ -140,8 +141,11 @@ __host__ __device__ inline TilePoint strip_point(const StripTiles &m, int tile, 
   P.active = tid < pts && q < qend;
   P.i1 = (int)(q / w);
   P.i2 = c0 + (int)(q % w);
-  P.ca = (int)((q0 / w + (qend - 1) / w) / 2);
+  const int r0 = (int)(q0 / w), r1 = (int)((qend - 1) / w);
+  P.ca = (r0 + r1) / 2;
   P.cb = c0 + w / 2;
+  P.ra = r1 - P.ca > P.ca - r0 ? r1 - P.ca : P.ca - r0;
+  P.rb = c0 + w - 1 - P.cb > P.cb - c0 ? c0 + w - 1 - P.cb : P.cb - c0;
   return P;
 }
 
@@ -171,6 +175,25 @@ __device__ inline Anchor make_anchor(const double Oc[3], const double *xp, const
   return a;
 }
 
+// What the anchor expansion of D_j - D_c leaves out, bounded for one trajectory point at distance
+// D_c = 1/invD from a tile whose points lie within dmax of the anchor with |n_c . Delta| <= gmax:
+// with h = |Delta|^2 - g^2, D_j - D_c = g + h/(2 D_c) - g h/(2 D_c^2) - h (|Delta|^2 - 5 g^2)/(8 D_c^3)
+// + ...; the tiles keep the first two terms.  Returned (in metres): the third-order term's bound plus
+// twice the fourth's, which covers the orders after it while dmax < D_c / 2.
+__device__ __forceinline__ double expansion_rest(double invD, double dmax, double gmax) {
+  const double d2 = dmax * dmax, i2 = invD * invD;
+  return 0.5 * gmax * d2 * i2 + 0.25 * d2 * (d2 + 4.0 * gmax * gmax) * i2 * invD;
+}
+
+// Limits of the expansion, per term: the phase error it leaves (radians, systematic), the rounding of
+// the FP32 phase (radians: its magnitude in turns times 2^-24), and the relative error of the
+// first-order 1/D_j.  A sub-tile that any trajectory point's bound exceeds is summed with exact FP64
+// geometry per term instead.
+constexpr double kRestPhase = 2e-6, kRoundPhase = 2e-5, kRestAmp = 1e-7;
+// The power density's limits: relative errors of (1 - n.beta)^-5 from the expansion's rest and from
+// the FP32 rounding of n_c . Delta.
+constexpr double kRestPd = 1e-6, kRoundPd = 1e-5;
+
 
 // Packed FP32x2 arithmetic (sm_100): one instruction performs the same operation on two values, each
 // rounded as the scalar operation would be.
@@ -194,6 +217,44 @@ struct FluxShared {
   float4 r[2][kFluxFields / 2][kSub / 2];  // double-buffered: sub-tile k in r[k & 1]
 };
 
+// The flux terms of grid point (i1, i2) and trajectory points [base, base + cnt) with the geometry in
+// FP64 per term (as the point-list kernel: R, 1/|R| from an FP32 reciprocal square root and two
+// Newton steps, the retarded phase in turns reduced exactly, beta - n), the amplitude, sincos and
+// sums in FP32; added to E (the field, not its negative).  For sub-tiles the anchor expansion does
+// not reach (coarse grids, near distances).
+__device__ __forceinline__ void flux_exact_terms(const double *__restrict__ xp, const double *__restrict__ bp,
+                                              int64_t n, double dt, const srs_grid2d &g, int i1, int i2,
+                                              double omega, int64_t base, int cnt, double E[6]) {
+  double Pq[3];
+  for (int c = 0; c < 3; ++c) Pq[c] = (g.origin[c] + g.u1[c] * (double)i1) + g.u2[c] * (double)i2;
+  const double wt = omega * 0.15915494309189535, inv_c = 1.0 / kC;
+  const float kap = (float)(-kC / omega), two_pi_f = 6.28318530717958647692f;
+  float e0 = 0, e1 = 0, e2 = 0, e3 = 0, e4 = 0, e5 = 0;
+  for (int k = 0; k < cnt; ++k) {
+    const int64_t i = base + k;
+    const double Rx = Pq[0] - __ldg(xp + i), Ry = Pq[1] - __ldg(xp + n + i), Rz = Pq[2] - __ldg(xp + 2 * n + i);
+    const double R2 = fma(Rx, Rx, fma(Ry, Ry, Rz * Rz));
+    const float yf = rsqrtf((float)R2);
+    double y = (double)yf;
+    double r = fma(-R2 * y, y, 1.0);
+    y = fma(0.5 * y, r, y);
+    r = fma(-R2 * y, y, 1.0);
+    y = fma(0.5 * y, r, y);  // 1/|R| to FP64 accuracy
+    const double ph = wt * fma(R2 * y, inv_c, dt * (double)i);
+    const float fr = (float)(ph - rint(ph));
+    const double nz = Rz * y;
+    const float ax = (float)(__ldg(bp + i) - Rx * y) * yf, ay = (float)(__ldg(bp + n + i) - Ry * y) * yf,
+                az = (float)(__ldg(bp + 2 * n + i) - nz) * yf;  // (beta - n)/D
+    const float cz = kap * (float)nz * (yf * yf);              // near field: i kap n_z / D^2
+    float sn, cs;
+    __sincosf(fr * two_pi_f, &sn, &cs);
+    e0 = fmaf(ax, cs, e0); e1 = fmaf(ax, sn, e1);
+    e2 = fmaf(ay, cs, e2); e3 = fmaf(ay, sn, e3);
+    e4 = fmaf(az, cs, fmaf(-cz, sn, e4)); e5 = fmaf(az, sn, fmaf(cz, cs, e5));
+  }
+  E[0] += e0; E[1] += e1; E[2] += e2; E[3] += e3; E[4] += e4; E[5] += e5;
+}
+
 // Flux: one strip tile (tile index `tile` of map m) against trajectory points [i0, iend); writes the six
 // partial sums (Re/Im of E_x, E_y, E_z without the final constant) of every point of the tile to
 // out6[c * np + j].
@@ -215,10 +276,15 @@ __device__ __forceinline__ void flux_tile(const double *__restrict__ xp, const d
   const bool active = P.active;
   const int da = P.i1 - P.ca, db = P.i2 - P.cb;
   const double wc = omega / kC;
+  // the tile's reach from its anchor (a bound on |Delta|)
+  const double dmax = P.ra * sqrt(g.u1[0] * g.u1[0] + g.u1[1] * g.u1[1] + g.u1[2] * g.u1[2]) +
+                      P.rb * sqrt(g.u2[0] * g.u2[0] + g.u2[1] * g.u2[1] + g.u2[2] * g.u2[2]);
   double E[6] = {0, 0, 0, 0, 0, 0};
 
-  // the records of trajectory points [base, base + kSub) into buffer b
-  auto fill = [&](int b, int64_t base) {
+  // the records of trajectory points [base, base + kSub) into buffer b; returns whether this thread's
+  // point needs the exact sum (the expansion's limits exceeded)
+  auto fill = [&](int b, int64_t base) -> int {
+    int bad = 0;
     float *rec = &sh.r[b][0][0].x;
     auto put = [&](int t, int f, float v) { rec[((f >> 1) * (kSub / 2) + (t >> 1)) * 4 + (f & 1) * 2 + (t & 1)] = v; };
     const int cnt = (int)imin64(kSub, iend - base);
@@ -229,9 +295,19 @@ __device__ __forceinline__ void flux_tile(const double *__restrict__ xp, const d
       const Anchor A = make_anchor(Oc, xp, bp, n, i);
       const double tau = dt * (double)i + A.Dc / kC;
       const double inv2pi = 0.15915494309189535;  // 1/(2 pi)
+      const double nu1 = A.nc[0] * g.u1[0] + A.nc[1] * g.u1[1] + A.nc[2] * g.u1[2];
+      const double nu2 = A.nc[0] * g.u2[0] + A.nc[1] * g.u2[1] + A.nc[2] * g.u2[2];
       put(tid, 0, (float)(reduce_2pi(omega * tau) * inv2pi));
-      put(tid, 1, (float)(reduce_2pi(wc * (A.nc[0] * g.u1[0] + A.nc[1] * g.u1[1] + A.nc[2] * g.u1[2])) * inv2pi));
-      put(tid, 2, (float)(reduce_2pi(wc * (A.nc[0] * g.u2[0] + A.nc[1] * g.u2[1] + A.nc[2] * g.u2[2])) * inv2pi));
+      put(tid, 1, (float)(reduce_2pi(wc * nu1) * inv2pi));
+      put(tid, 2, (float)(reduce_2pi(wc * nu2) * inv2pi));
+      {
+        const double gmax = P.ra * fabs(nu1) + P.rb * fabs(nu2);
+        const double curv = 0.5 * dmax * dmax * A.invDc;  // |h|/(2 D_c) <= this, metres
+        const double turns = (wc * curv) * inv2pi + 0.5 * (1 + P.ra + P.rb);
+        const double ramp = (gmax + curv) * A.invDc;       // |D_j - D_c| / D_c
+        bad = wc * expansion_rest(A.invDc, dmax, gmax) > kRestPhase ||
+              turns * (6.283185307179586 * 0x1p-24) > kRoundPhase || ramp * ramp > kRestAmp;
+      }
       put(tid, 3, (float)(-wc * 0.5 * A.invDc * inv2pi));
       put(tid, 4, (float)A.nc[0]);
       put(tid, 5, (float)A.nc[1]);
@@ -247,17 +323,22 @@ __device__ __forceinline__ void flux_tile(const double *__restrict__ xp, const d
       // the odd count's partner slot: all zero, so 1/D_j = 0 and its amplitude and near-field term vanish
       for (int f = 0; f < kFluxFields; ++f) put(tid, f, 0.0f);
     }
+    return bad;
   };
 
   __syncthreads();  // the caller's previous use of sh is over
-  if (i0 < iend) fill(0, i0);
+  int bad_cur = i0 < iend ? fill(0, i0) : 0;
   int b = 0;
   for (int64_t base = i0; base < iend; base += kSub, b ^= 1) {
     const int cnt = (int)imin64(kSub, iend - base);
     // records of this sub-tile complete; every thread is done with the other buffer
-    __syncthreads();
-    if (base + kSub < iend) fill(b ^ 1, base + kSub);
+    const int exact = __syncthreads_or(bad_cur);
+    bad_cur = base + kSub < iend ? fill(b ^ 1, base + kSub) : 0;
     if (!active) continue;
+    if (exact) {
+      flux_exact_terms(xp, bp, n, dt, g, P.i1, P.i2, omega, base, cnt, E);
+      continue;
+    }
     // this thread's offset from the anchor point (formed here, after the FP64 anchors, so that it does
     // not occupy registers while they are computed)
     float Dl[3];

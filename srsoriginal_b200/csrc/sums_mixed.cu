@@ -99,6 +99,9 @@ __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__r
   const double *xp = X + off, *bp = Bt + off, *ap = Ac + off;
   const int64_t i0 = (int64_t)s * chunk, iend = imin64(n, i0 + chunk);
   const int da = P.i1 - P.ca, db = P.i2 - P.cb;
+  // the tile's reach from its anchor (a bound on |Delta|)
+  const double dmax = P.ra * sqrt(g.u1[0] * g.u1[0] + g.u1[1] * g.u1[1] + g.u1[2] * g.u1[2]) +
+                      P.rb * sqrt(g.u2[0] * g.u2[0] + g.u2[1] * g.u2[1] + g.u2[2] * g.u2[2]);
   double omb_ref;
   {
     const double bx = bp[0], by = bp[n], bz = bp[2 * n];
@@ -106,7 +109,12 @@ __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__r
     omb_ref = (1.0 - b2) / (1.0 + sqrt(b2));
   }
 
-  auto fill = [&](int buf, int64_t base) {
+  // the records of trajectory points [base, base + kSub) into buffer buf; returns whether this thread's
+  // point needs the exact sum.  An error e in D_j - D_c moves n.beta by ~e/D_c, which (1 - n.beta)^-5
+  // amplifies by 5/(1 - |beta|) relative: the expansion's rest and the FP32 rounding of n_c . Delta are
+  // bounded in those terms.
+  auto fill = [&](int buf, int64_t base) -> int {
+    int bad = 0;
     float *rec = &sm[buf][0][0].x;
     auto put = [&](int t, int f, float v) { rec[((f >> 1) * (kSub / 2) + (t >> 1)) * 4 + (f & 1) * 2 + (t & 1)] = v; };
     const int cnt = (int)imin64(kSub, iend - base);
@@ -115,6 +123,15 @@ __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__r
       double Oc[3];
       for (int c = 0; c < 3; ++c) Oc[c] = g.origin[c] + (double)P.ca * g.u1[c] + (double)P.cb * g.u2[c];
       const Anchor A = make_anchor(Oc, xp, bp, n, i);
+      {
+        const double nu1 = A.nc[0] * g.u1[0] + A.nc[1] * g.u1[1] + A.nc[2] * g.u1[2];
+        const double nu2 = A.nc[0] * g.u2[0] + A.nc[1] * g.u2[1] + A.nc[2] * g.u2[2];
+        const double gmax = P.ra * fabs(nu1) + P.rb * fabs(nu2);
+        const double gain = 5.0 * A.invDc / A.omb;
+        const double ramp = (gmax + 0.5 * dmax * dmax * A.invDc) * A.invDc;
+        bad = gain * expansion_rest(A.invDc, dmax, gmax) > kRestPd || gain * gmax * 0x1p-24 > kRoundPd ||
+              ramp * ramp > kRestAmp;
+      }
       const double ax = ap[i], ay = ap[n + i], az = ap[2 * n + i];
       const double r = omb_ref / A.omb;
       put(tid, 0, (float)A.nc[0]); put(tid, 1, (float)A.nc[1]); put(tid, 2, (float)A.nc[2]);
@@ -135,16 +152,56 @@ __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__r
       // 1 - n.beta finite
       for (int f = 0; f < kPdFields; ++f) put(tid, f, f == 11 ? -1.0f : 0.0f);
     }
+    return bad;
   };
 
   double sum = 0;
-  if (i0 < iend) fill(0, i0);
+  int bad_cur = i0 < iend ? fill(0, i0) : 0;
   int buf = 0;
   for (int64_t base = i0; base < iend; base += kSub, buf ^= 1) {
     const int cnt = (int)imin64(kSub, iend - base);
-    __syncthreads();  // records of this sub-tile complete; every thread is done with the other buffer
-    if (base + kSub < iend) fill(buf ^ 1, base + kSub);
+    // records of this sub-tile complete; every thread is done with the other buffer
+    const int exact = __syncthreads_or(bad_cur);
+    bad_cur = base + kSub < iend ? fill(buf ^ 1, base + kSub) : 0;
     if (!active) continue;
+    if (exact) {
+      // FP64 geometry per term (R, 1/|R|, n, n - beta), the rest from the records, as the point-list kernel
+      const float *rec = &sm[buf][0][0].x;
+      auto get = [&](int f, int k) { return rec[((f >> 1) * (kSub / 2) + (k >> 1)) * 4 + (f & 1) * 2 + (k & 1)]; };
+      double Pq[3];
+      for (int c = 0; c < 3; ++c) Pq[c] = (g.origin[c] + g.u1[c] * (double)P.i1) + g.u2[c] * (double)P.i2;
+      const float nrx = (float)nx_, nry = (float)ny_, nrz = (float)nz_;
+      float acc = 0.f;
+      for (int k = 0; k < cnt; ++k) {
+        const int64_t i = base + k;
+        const double Rx = Pq[0] - __ldg(xp + i), Ry = Pq[1] - __ldg(xp + n + i), Rz = Pq[2] - __ldg(xp + 2 * n + i);
+        const double R2 = fma(Rx, Rx, fma(Ry, Ry, Rz * Rz));
+        const float yf = rsqrtf((float)R2);
+        double y = (double)yf;
+        double e = fma(-R2 * y, y, 1.0);
+        y = fma(0.5 * y, e, y);
+        e = fma(-R2 * y, y, 1.0);
+        y = fma(0.5 * y, e, y);  // 1/|R| to FP64 accuracy
+        const double nx = Rx * y, ny = Ry * y, nz = Rz * y;
+        const float mx = (float)(nx - __ldg(bp + i)), my = (float)(ny - __ldg(bp + n + i)),
+                    mz = (float)(nz - __ldg(bp + 2 * n + i));  // n - beta
+        const float dx = mx - get(8, k), dy = my - get(9, k), dz = mz - get(10, k);  // n - bhat
+        const float nd = fmaf((float)nz, nrz, fmaf((float)ny, nry, (float)nx * nrx));
+        const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        const float opn = fmaf(get(15, k), d2, 1.0f);
+        const float opnbn = get(11, k) * opn;  // -(1 - n.beta)
+        const float acx = get(12, k), acy = get(13, k), acz = get(14, k);
+        const float na = fmaf(dz, acz, fmaf(dy, acy, fmaf(dx, acx, get(16, k))));
+        const float Vx = fmaf(mx, na, acx * opnbn), Vy = fmaf(my, na, acy * opnbn), Vz = fmaf(mz, na, acz * opnbn);
+        const float v2 = fmaf(Vz, Vz, fmaf(Vy, Vy, Vx * Vx));
+        const float o2 = opn * opn, o5 = o2 * o2 * opn;
+        float term = v2 * (yf * yf) * nd * get(17, k) * __fdividef(1.0f, o5);
+        if (directional && !(nd > 0.0f)) term = 0.0f;
+        acc += term;
+      }
+      sum += (double)acc;
+      continue;
+    }
     // this thread's offset from the anchor point (formed after the FP64 anchors, off their registers)
     float Dl[3];
     for (int c = 0; c < 3; ++c) Dl[c] = (float)((double)da * g.u1[c] + (double)db * g.u2[c]);

@@ -579,3 +579,35 @@ def test_mixed_grid_tiles_ragged_shapes(n1, n2):
     torch.cuda.synchronize()
     assert np.all(np.isfinite(a.cpu().numpy()))
     assert_mixed(a.cpu().numpy(), c.cpu().numpy())
+
+
+@pytest.mark.parametrize("n,width,z,energy", [(41, 0.05, 30.0, 1000.0), (41, 0.05, 10.0, 1000.0), (21, 0.05, 10.0, 1000.0),
+                                              (51, 0.02, 5.0, 500.0), (31, 0.1, 30.0, 456.0), (21, 0.1, 3.0, 456.0)])
+def test_mixed_grid_coarse_and_near_maps(n, width, z, energy):
+    """Coarse grids and near screens, where the tiles' anchor expansion would leave phase errors of
+    1e-3 rad and more: every anchor bounds what the expansion leaves out, and those sub-tiles are
+    summed with exact FP64 geometry per term.  The flux is held to the point-list mixed kernel (FP64
+    geometry for every term) and to normwise 1e-5 of FP64.  At 1 keV the retarded phase w (t + D/c) is
+    ~1e11 rad, whose FP64 rounding (~1e-5 rad per term, in the FP64 kernel as in any other evaluation)
+    moves the weakest points of such a map by up to ~1e-3 between two correct evaluations: there the
+    max relative error at 1e-3 of the maximum may exceed 1e-4, but not the point-list kernel's."""
+    import torch
+    from srsoriginal_b200 import _lib, device as D
+    from srsoriginal_b200.sr import rectangle_points
+    tr = reference_trajectory_on_device(20001)
+    xyz, _, nrm, grid = rectangle_points([n, n], "XY", [width, width], translation=[0, 0, z])
+    m = n * n
+    pts = torch.as_tensor(np.ascontiguousarray(xyz.reshape(-1)), device="cuda")
+    nrms = torch.as_tensor(np.ascontiguousarray(np.tile(nrm, (m, 1)).reshape(-1)), device="cuda")
+    a, c, q = (torch.empty(m, dtype=torch.float64, device="cuda") for _ in range(3))
+    D.flux(tr, -O.QE, 0.5, energy, a, grid=grid, precision=_lib.MIXED)
+    D.flux(tr, -O.QE, 0.5, energy, q, points=pts, precision=_lib.MIXED)
+    D.flux(tr, -O.QE, 0.5, energy, c, points=pts, precision=_lib.FP64)
+    torch.cuda.synchronize()
+    mx, nrm = rel_err(a.cpu().numpy(), c.cpu().numpy(), 1e-3)
+    mq, _ = rel_err(q.cpu().numpy(), c.cpu().numpy(), 1e-3)
+    assert nrm <= TOL_MIXED_NORM and mx <= max(TOL_MIXED, 1.5 * mq), (mx, mq, nrm)
+    D.power_density(tr, -O.QE, 0.5, a, grid=grid, precision=_lib.MIXED)
+    D.power_density(tr, -O.QE, 0.5, c, points=pts, normals=nrms, precision=_lib.FP64)
+    torch.cuda.synchronize()
+    assert_mixed(a.cpu().numpy(), c.cpu().numpy())
