@@ -89,11 +89,14 @@ struct Scratch {
   double *diag;            // [it]: largest mismatch of iteration it (relative to the scales)
   double *rmax;            // this launch's largest interior mismatch (reset by the last block)
   int *flags;              // [0] converged, [1] iterations, [2] near, [3] the last pass stored, [4] ticket
+  Prepared *prep;          // [nfields]: the fields' constants, computed once by the init kernel
   double scale_pos, scale_vel;
 };
 
-__global__ void shoot_init_kernel(Plan P, const srs_particle *__restrict__ part, Scratch W) {
+__global__ void shoot_init_kernel(Plan P, const srs_particle *__restrict__ part, Scratch W,
+                                  const srs_field *__restrict__ fields, int nfields) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < nfields) prepare(fields[g], W.prep[g]);  // once per integration, not once per pass and block
   if (g == 0) {
     for (int k = 0; k < 5; ++k) W.flags[k] = 0;
     for (int k = 0; k < kMaxIters; ++k) W.diag[k] = 0.0;
@@ -166,7 +169,7 @@ __device__ __forceinline__ void shoot_pass(PassShared<kShootThreads / G> &sh, co
   const unsigned full = 0xffffffffu;
   for (int i = t; i < nfields; i += blockDim.x) {
     sf[i] = gfields[i];
-    prepare(sf[i], sp[i]);
+    sp[i] = W.prep[i];
   }
   // (1) this chunk's start states: the previous iteration's update, segment after segment (the first
   // segment's was set by the last block's sweep)
@@ -511,6 +514,7 @@ Scratch carve(void *scratch, const Plan &P) {
   s.diag = s.dstart + 6 * chunks;
   s.rmax = s.diag + kMaxIters;
   s.flags = reinterpret_cast<int *>(s.rmax + 1);
+  s.prep = reinterpret_cast<Prepared *>(s.rmax + 5);  // after the 5 flags, 8-byte aligned
   s.scale_pos = s.scale_vel = 1.0;
   return s;
 }
@@ -559,7 +563,8 @@ int shoot_default_steps(int64_t nsteps) {
 size_t shoot_scratch_bytes(int64_t nfwd, int64_t nbwd, int steps_per_segment, int nfields) {
   const Plan P = make_plan(nfwd, nbwd, 1.0, steps_per_segment, nfields);
   const size_t segs = (size_t)(P.sfp + P.sbp) + 1, chunks = (size_t)(P.sfp + P.sbp) / P.m + 1;
-  return sizeof(double) * (segs * 48 + chunks * (kChunkDoubles + 6) + kMaxIters + 1) + 64;
+  return sizeof(double) * (segs * 48 + chunks * (kChunkDoubles + 6) + kMaxIters + 1) + 64 +
+         sizeof(Prepared) * (size_t)nfields;
 }
 
 cudaError_t launch_rk4_shoot(const srs_field *d_fields, int nfields, const srs_particle *d_particle,
@@ -585,7 +590,7 @@ cudaError_t launch_rk4_shoot(const srs_field *d_fields, int nfields, const srs_p
   // dynamic shared memory: the grid samples during the integration, the chunk maps in the sweep
   const size_t smem = sizeof(double) * (size_t)std::max<int64_t>(stage_doubles, (int64_t)(segs / P.m) * kChunkDoubles);
   const int G = lanes_for(nfields), blocks = segs / P.m;
-  shoot_init_kernel<<<(segs + 127) / 128, 128, 0, s>>>(P, d_particle, W);
+  shoot_init_kernel<<<(std::max(segs, nfields) + 127) / 128, 128, 0, s>>>(P, d_particle, W, d_fields, nfields);
   for (int it = 0; it < iters; ++it)
     if (cudaError_t e = launch_pass_g(G, blocks, smem, s, d_fields, nfields, d_particle, P, W, d_x, d_b, d_a,
                                       stage_doubles, 0))
