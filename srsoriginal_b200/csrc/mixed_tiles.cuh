@@ -180,7 +180,7 @@ __device__ inline Anchor make_anchor(const double Oc[3], const double *xp, const
 // with h = |Delta|^2 - g^2, D_j - D_c = g + h/(2 D_c) - g h/(2 D_c^2) - h (|Delta|^2 - 5 g^2)/(8 D_c^3)
 // + ...; the tiles keep the first two terms.  Returned (in metres): the third-order term's bound plus
 // twice the fourth's, which covers the orders after it while dmax < D_c / 2.
-__device__ __forceinline__ double expansion_rest(double invD, double dmax, double gmax) {
+__host__ __device__ __forceinline__ double expansion_rest(double invD, double dmax, double gmax) {
   const double d2 = dmax * dmax, i2 = invD * invD;
   return 0.5 * gmax * d2 * i2 + 0.25 * d2 * (d2 + 4.0 * gmax * gmax) * i2 * invD;
 }

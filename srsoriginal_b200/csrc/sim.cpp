@@ -473,8 +473,16 @@ struct srs_sim {
       } else if (srs_status st = trajectories(&ps[b0], np, X, B, A, view)) {
         return st;
       }
-      SRS_CUDA(vals.alloc(sizeof(double) * (size_t)nout * np, stream));
       srs_beam_consts bc{ps[b0].q, ps[b0].current};
+      // one particle with weight 1 into outputs that start from zero: its sums are the result (a
+      // compensated add of v to zero gives v), so they are written straight into the output
+      if (fresh && ps.size() == 1 && weight == 1.0) {
+        if (srs_status st = sum(view, bc, d_out)) return st;
+        uploaded = true;
+        b0 = b1;
+        continue;
+      }
+      SRS_CUDA(vals.alloc(sizeof(double) * (size_t)nout * np, stream));
       if (srs_status st = sum(view, bc, vals.as<double>())) return st;
       if (!uploaded)
         if (srs_status st = upload()) return st;

@@ -1,0 +1,31 @@
+"""Host-side checks of the mixed grid kernels' strip tiles and expansion error bound
+(tests/tiles_check.cu, compiled here with nvcc and run on the CPU; no GPU is used)."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    return None
+
+
+def test_strip_tiles_and_expansion_bound(tmp_path):
+    nvcc = _nvcc()
+    if nvcc is None:
+        pytest.skip("nvcc not found")
+    exe = tmp_path / "tiles_check"
+    cmd = [nvcc, "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a",
+           "-I", os.path.join(ROOT, "srsoriginal_b200", "csrc"), "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "tiles_check.cu"), "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "tiles 0 bound 0" in r.stdout
