@@ -179,7 +179,8 @@ __device__ inline Anchor make_anchor(const double Oc[3], const double *xp, const
 // D_c = 1/invD from a tile whose points lie within dmax of the anchor with |n_c . Delta| <= gmax:
 // with h = |Delta|^2 - g^2, D_j - D_c = g + h/(2 D_c) - g h/(2 D_c^2) - h (|Delta|^2 - 5 g^2)/(8 D_c^3)
 // + ...; the tiles keep the first two terms.  Returned (in metres): the third-order term's bound plus
-// twice the fourth's, which covers the orders after it while dmax < D_c / 2.
+// twice the fourth's, which covers the orders after it while dmax < D_c / 2 (checked against the exact
+// rest on random geometries by tests/tiles_check.cu); callers treat dmax >= D_c / 2 as out of reach.
 __host__ __device__ __forceinline__ double expansion_rest(double invD, double dmax, double gmax) {
   const double d2 = dmax * dmax, i2 = invD * invD;
   return 0.5 * gmax * d2 * i2 + 0.25 * d2 * (d2 + 4.0 * gmax * gmax) * i2 * invD;
@@ -305,7 +306,7 @@ __device__ __forceinline__ void flux_tile(const double *__restrict__ xp, const d
         const double curv = 0.5 * dmax * dmax * A.invDc;  // |h|/(2 D_c) <= this, metres
         const double turns = (wc * curv) * inv2pi + 0.5 * (1 + P.ra + P.rb);
         const double ramp = (gmax + curv) * A.invDc;       // |D_j - D_c| / D_c
-        bad = wc * expansion_rest(A.invDc, dmax, gmax) > kRestPhase ||
+        bad = dmax * A.invDc >= 0.5 || wc * expansion_rest(A.invDc, dmax, gmax) > kRestPhase ||
               turns * (6.283185307179586 * 0x1p-24) > kRoundPhase || ramp * ramp > kRestAmp;
       }
       put(tid, 3, (float)(-wc * 0.5 * A.invDc * inv2pi));

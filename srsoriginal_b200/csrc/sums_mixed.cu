@@ -129,8 +129,8 @@ __global__ void __launch_bounds__(kThreads, 5) pd_mixed_kernel(const double *__r
         const double gmax = P.ra * fabs(nu1) + P.rb * fabs(nu2);
         const double gain = 5.0 * A.invDc / A.omb;
         const double ramp = (gmax + 0.5 * dmax * dmax * A.invDc) * A.invDc;
-        bad = gain * expansion_rest(A.invDc, dmax, gmax) > kRestPd || gain * gmax * 0x1p-24 > kRoundPd ||
-              ramp * ramp > kRestAmp;
+        bad = dmax * A.invDc >= 0.5 || gain * expansion_rest(A.invDc, dmax, gmax) > kRestPd ||
+              gain * gmax * 0x1p-24 > kRoundPd || ramp * ramp > kRestAmp;
       }
       const double ax = ap[i], ay = ap[n + i], az = ap[2 * n + i];
       const double r = omb_ref / A.omb;
