@@ -1,4 +1,4 @@
-"""Host-side checks of the mixed grid kernels' strip tiles and expansion error bound
+"""Host-side checks of the mixed grid kernels' strip tiles, expansion error bound and trajectory chunks
 (tests/tiles_check.cu, compiled here with nvcc and run on the CPU; no GPU is used)."""
 import os
 import shutil
@@ -28,4 +28,4 @@ def test_strip_tiles_and_expansion_bound(tmp_path):
     assert r.returncode == 0, r.stderr[-2000:]
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
-    assert "tiles 0 bound 0" in r.stdout
+    assert "tiles 0 bound 0 chunks 0" in r.stdout

@@ -6,6 +6,7 @@
 //   2. Random geometries: the exact rest of D_j - D_c after its first two terms, computed in long
 //      double from the cancellation-free form (2 g D_c + |Delta|^2)/(D_j + D_c), never exceeds
 //      expansion_rest for the tile's reach, while dmax < D_c / 2.
+//   3. Trajectory chunks of the launchers (aligned_chunk, used_chunks, splits_for).
 #include <cmath>
 #include <cstdio>
 #include <random>
@@ -88,8 +89,29 @@ static int check_bound() {
   return bad + (tried < 1000);
 }
 
+// 3. Trajectory chunking: for every split count the launchers can ask for, whole sub-tiles per chunk,
+//    every point in exactly one chunk, no more chunks than asked for; the split model's choice is
+//    within its range.
+static int check_chunks() {
+  int bad = 0;
+  for (int64_t n : {1, 2, 127, 128, 129, 2001, 20001, 40001, 100000}) {
+    for (int S = 1; S <= 300; ++S) {
+      const int64_t chunk = aligned_chunk(n, S);
+      const int used = used_chunks(n, chunk);
+      if (chunk % kSub != 0 || chunk < kSub || used > S || used < 1 || (int64_t)(used - 1) * chunk >= n ||
+          (int64_t)used * chunk < n)
+        ++bad;
+    }
+    for (int64_t ctas : {1, 7, 81, 318, 1024, 100000}) {
+      const int s = splits_for(ctas, n, 256, 888);
+      if (s < 1 || s > std::max<int64_t>(1, n / 256)) ++bad;
+    }
+  }
+  return bad;
+}
+
 int main() {
-  const int a = check_tiles(), b = check_bound();
-  std::printf("tiles %d bound %d\n", a, b);
-  return a + b != 0;
+  const int a = check_tiles(), b = check_bound(), c = check_chunks();
+  std::printf("tiles %d bound %d chunks %d\n", a, b, c);
+  return a + b + c != 0;
 }
