@@ -80,6 +80,10 @@ def lib():
                                C.c_double, C.c_double, _D, _D]
     L.orc_flux.argtypes = [_D, _D, C.c_int64, C.c_double, _D, C.c_int64, C.c_double, C.c_double,
                            C.c_double, C.c_double, _D, _D]
+    L.orc_flux_exact.argtypes = [_D, _D, C.c_int64, C.c_double, _D, C.c_int64, C.c_double, C.c_double,
+                                 C.c_double, _D]
+    L.orc_spectrum_exact.argtypes = [_D, _D, C.c_int64, C.c_double, _D, _D, C.c_int64, C.c_double,
+                                     C.c_double, _D]
     L.orc_power_density.argtypes = [_D, _D, _D, C.c_int64, C.c_double, _D, _D, C.c_int64, C.c_int,
                                     C.c_double, C.c_double, _D, _D]
     L.orc_total_power.argtypes = [_D, _D, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double]
@@ -243,6 +247,26 @@ def flux(X, B, dt, points, energy_ev, charge, current, weight=1.0, out=None, com
     comp = np.zeros(len(P)) if comp is None else comp
     lib().orc_flux(_p(X), _p(B), X.shape[1], dt, _p(P), len(P), energy_ev, charge, current, weight,
                    _p(out), _p(comp))
+    return out
+
+
+def flux_exact(X, B, dt, points, energy_ev, charge, current):
+    """The flux sum of flux() evaluated in long double (the exact value FP64 evaluations approximate)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    P = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros(len(P))
+    lib().orc_flux_exact(_p(X), _p(B), X.shape[1], dt, _p(P), len(P), energy_ev, charge, current, _p(out))
+    return out
+
+
+def spectrum_exact(X, B, dt, obs, energies, charge, current):
+    """The spectrum sum of spectrum() evaluated in long double."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    e = np.ascontiguousarray(energies, dtype=np.float64)
+    out = np.zeros(len(e))
+    lib().orc_spectrum_exact(_p(X), _p(B), X.shape[1], dt, _v3(obs), _p(e), len(e), charge, current, _p(out))
     return out
 
 

@@ -76,6 +76,13 @@ void orc_power_density(const double *x, const double *b, const double *a, int64_
 double orc_total_power(const double *b, const double *a, int64_t n, double dt, double charge,
                        double current, double gamma);
 
+/* The same flux / spectrum sums in long double on the same FP64 inputs (written, not added): the exact
+ * values that FP64 evaluations of the retarded phase approximate (see srs_oracle.c). */
+void orc_flux_exact(const double *x, const double *b, int64_t n, double dt, const double *points, int64_t np,
+                    double energy_ev, double charge, double current, double *out);
+void orc_spectrum_exact(const double *x, const double *b, int64_t n, double dt, const double obs[3],
+                        const double *energies_ev, int64_t ne, double charge, double current, double *out);
+
 /* Spectrum energy grid (TSpectrumContainer::Init(N, EFirst, ELast)). */
 void orc_energy_grid(int64_t n, double efirst, double elast, double *out);
 
