@@ -590,7 +590,8 @@ def test_mixed_grid_coarse_and_near_maps(n, width, z, energy):
     geometry for every term) and to normwise 1e-5 of FP64.  At 1 keV the retarded phase w (t + D/c) is
     ~1e11 rad, whose FP64 rounding (~1e-5 rad per term, in the FP64 kernel as in any other evaluation)
     moves the weakest points of such a map by up to ~1e-3 between two correct evaluations: there the
-    max relative error at 1e-3 of the maximum may exceed 1e-4, but not the point-list kernel's."""
+    max relative error at 1e-3 of the maximum may exceed 1e-4, but not 1.5 x the point-list kernel's
+    nor 1e-3."""
     import torch
     from srsoriginal_b200 import _lib, device as D
     from srsoriginal_b200.sr import rectangle_points
@@ -606,7 +607,8 @@ def test_mixed_grid_coarse_and_near_maps(n, width, z, energy):
     torch.cuda.synchronize()
     mx, nrm = rel_err(a.cpu().numpy(), c.cpu().numpy(), 1e-3)
     mq, _ = rel_err(q.cpu().numpy(), c.cpu().numpy(), 1e-3)
-    assert nrm <= TOL_MIXED_NORM and mx <= max(TOL_MIXED, 1.5 * mq), (mx, mq, nrm)
+    # relative to the point-list kernel, and never above 1e-3 whatever that kernel does
+    assert nrm <= TOL_MIXED_NORM and mx <= min(1e-3, max(TOL_MIXED, 1.5 * mq)), (mx, mq, nrm)
     D.power_density(tr, -O.QE, 0.5, a, grid=grid, precision=_lib.MIXED)
     D.power_density(tr, -O.QE, 0.5, c, points=pts, normals=nrms, precision=_lib.FP64)
     torch.cuda.synchronize()
