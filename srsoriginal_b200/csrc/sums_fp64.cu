@@ -11,6 +11,13 @@
 // reduced modulo 2*pi (Cody-Waite, three-part 2*pi, FMA) before the FP64 sincos, which is then
 // evaluated on |r| <= pi.
 //
+// Divisions: every division of a term by the same distance D (or D^2, or (1 - n.beta)^5) is formed
+// from one correctly rounded reciprocal (__drcp_rn) by Markstein's correction (div_rn), which gives
+// the correctly rounded quotient, i.e. the IEEE division's result bit for bit, in three instructions
+// instead of a division sequence each (normal operands: D, 1/D and the quotients of these sums are far
+// from overflow and underflow).  The power density's (1 - n.beta)^5 is formed by multiplications
+// (x^2 x^2 x, within two ulps of the reference's std::pow(x, 5)).
+//
 // Parallel layout (B200: 148 SMs): one thread per output (energy or observation point), 128 outputs
 // per CTA, and the trajectory axis split into S contiguous chunks across CTAs so that small outputs
 // (1000 energies) still fill every SM.  Each CTA stages its chunk through shared memory in 128-point
@@ -28,6 +35,16 @@ namespace srs {
 namespace {
 
 constexpr int kTile = 128;     // outputs per CTA and trajectory points per shared-memory tile
+
+// a / b for the three components, from rb = RN(1/b)
+__device__ __forceinline__ V3 div3_rn(V3 a, double b, double rb) {
+  return v3(div_rn(a.x, b, rb), div_rn(a.y, b, rb), div_rn(a.z, b, rb));
+}
+// a / |a| (TVector3D::UnitVector), the three divisions from one reciprocal
+__device__ __forceinline__ V3 unit_rn(V3 a) {
+  const double m = mag(a);
+  return div3_rn(a, m, __drcp_rn(m));
+}
 constexpr int kTargetCtas = 148 * 8;
 
 int choose_splits(int64_t ctas_without_split, int64_t n) {
@@ -51,7 +68,7 @@ __global__ void __launch_bounds__(kTile) flux_fp64_kernel(const double *__restri
   const int64_t i0 = (int64_t)s * chunk, i1 = imin64(n, i0 + chunk);
   const bool active = j < np;
   V3 obs = active ? v3(pts[3 * j], pts[3 * j + 1], pts[3 * j + 2]) : v3(0, 0, 1);
-  const double icow = kC / omega;
+  const double icow = kC / omega, rc = 1.0 / kC;
   double axr = 0, axi = 0, ayr = 0, ayi = 0, azr = 0, azi = 0;
   for (int64_t base = i0; base < i1; base += kTile) {
     const int cnt = (int)imin64(kTile, i1 - base);
@@ -68,17 +85,18 @@ __global__ void __launch_bounds__(kTile) flux_fp64_kernel(const double *__restri
     for (int k = 0; k < cnt; ++k) {
       V3 R = obs - v3(sx[0][k], sx[1][k], sx[2][k]);
       double m = mag(R);
-      V3 N = R / m;
-      double ph = omega * (dt * (double)(int)(base + k) + m / kC);
+      const double rm = __drcp_rn(m);
+      V3 N = div3_rn(R, m, rm);
+      double ph = omega * (dt * (double)(int)(base + k) + div_rn(m, kC, rc));
       double sn, cs;
       sincos(reduce_2pi(ph), &sn, &cs);
-      double f = icow / m;
+      double f = div_rn(icow, m, rm);
       double ar, ai;
-      ar = (sb[0][k] - N.x) / m; ai = -(N.x * f) / m;
+      ar = div_rn(sb[0][k] - N.x, m, rm); ai = div_rn(-(N.x * f), m, rm);
       axr += ar * cs - ai * sn; axi += ar * sn + ai * cs;
-      ar = (sb[1][k] - N.y) / m; ai = -(N.y * f) / m;
+      ar = div_rn(sb[1][k] - N.y, m, rm); ai = div_rn(-(N.y * f), m, rm);
       ayr += ar * cs - ai * sn; ayi += ar * sn + ai * cs;
-      ar = (sb[2][k] - N.z) / m; ai = -(N.z * f) / m;
+      ar = div_rn(sb[2][k] - N.z, m, rm); ai = div_rn(-(N.z * f), m, rm);
       azr += ar * cs - ai * sn; azi += ar * sn + ai * cs;
     }
   }
@@ -140,7 +158,7 @@ __global__ void __launch_bounds__(kTile) spectrum_fp64_kernel(const double *__re
                                                               int64_t ne, int64_t chunk,
                                                               double *__restrict__ partial) {
   // Per trajectory point (energy independent): n = R/|R|, D, tau = i*dt + D/c, (beta - n)/D.
-  __shared__ double sN[3][kTile], sD[kTile], sT[kTile], sA[3][kTile];
+  __shared__ double sN[3][kTile], sD[kTile], sR[kTile], sT[kTile], sA[3][kTile];
   const int tid = threadIdx.x;
   const int64_t k = (int64_t)blockIdx.x * kTile + tid;
   const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
@@ -157,27 +175,29 @@ __global__ void __launch_bounds__(kTile) spectrum_fp64_kernel(const double *__re
       const int64_t i = base + tid;
       V3 R = obs - v3(xp[i], xp[n + i], xp[2 * n + i]);
       double m = mag(R);
-      V3 N = R / m;
+      const double rm = __drcp_rn(m);
+      V3 N = div3_rn(R, m, rm);
       sN[0][tid] = N.x; sN[1][tid] = N.y; sN[2][tid] = N.z;
       sD[tid] = m;
-      sT[tid] = dt * (double)(int)i + m / kC;
-      sA[0][tid] = (bp[i] - N.x) / m;
-      sA[1][tid] = (bp[n + i] - N.y) / m;
-      sA[2][tid] = (bp[2 * n + i] - N.z) / m;
+      sR[tid] = rm;
+      sT[tid] = dt * (double)(int)i + div_rn(m, kC, 1.0 / kC);
+      sA[0][tid] = div_rn(bp[i] - N.x, m, rm);
+      sA[1][tid] = div_rn(bp[n + i] - N.y, m, rm);
+      sA[2][tid] = div_rn(bp[2 * n + i] - N.z, m, rm);
     }
     __syncthreads();
     if (!active) continue;
     for (int q = 0; q < cnt; ++q) {
-      const double m = sD[q];
+      const double m = sD[q], rm = sR[q];
       double sn, cs;
       sincos(reduce_2pi(omega * sT[q]), &sn, &cs);
-      const double f = icow / m;
+      const double f = div_rn(icow, m, rm);
       double ar, ai;
-      ar = sA[0][q]; ai = -(sN[0][q] * f) / m;
+      ar = sA[0][q]; ai = div_rn(-(sN[0][q] * f), m, rm);
       axr += ar * cs - ai * sn; axi += ar * sn + ai * cs;
-      ar = sA[1][q]; ai = -(sN[1][q] * f) / m;
+      ar = sA[1][q]; ai = div_rn(-(sN[1][q] * f), m, rm);
       ayr += ar * cs - ai * sn; ayi += ar * sn + ai * cs;
-      ar = sA[2][q]; ai = -(sN[2][q] * f) / m;
+      ar = sA[2][q]; ai = div_rn(-(sN[2][q] * f), m, rm);
       azr += ar * cs - ai * sn; azi += ar * sn + ai * cs;
     }
   }
@@ -227,17 +247,19 @@ __global__ void __launch_bounds__(kTile) pd_fp64_kernel(const double *__restrict
       const V3 Xk = v3(sx[0][k], sx[1][k], sx[2][k]);
       const V3 B = v3(sb[0][k], sb[1][k], sb[2][k]);
       const V3 AC = v3(sa[0][k], sa[1][k], sa[2][k]);
-      const V3 N1 = unit(obs - Xk);
-      const V3 N2 = unit(orthogonal(N1));
-      const V3 N3 = unit(cross(N1, N2));
+      const V3 N1 = unit_rn(obs - Xk);
+      const V3 N2 = unit_rn(orthogonal(N1));
+      const V3 N3 = unit_rn(cross(N1, N2));
       const double nd = dot(N1, nrm);
       if (directional && nd <= 0) continue;
       const V3 num = cross(N1, cross(N1 - B, AC));
-      const double den = pow(1 - dot(B, N1), 5.0);
+      const double omb = 1 - dot(B, N1), omb2 = omb * omb;
+      const double den = omb2 * omb2 * omb;
       const double p2 = dot(num, N2), p3 = dot(num, N3);
       const double m2 = mag2(obs - Xk);
-      sum += p2 * p2 / den / m2 * nd;
-      sum += p3 * p3 / den / m2 * nd;
+      const double rden = __drcp_rn(den), rm2 = __drcp_rn(m2);
+      sum += div_rn(div_rn(p2 * p2, den, rden), m2, rm2) * nd;
+      sum += div_rn(div_rn(p3 * p3, den, rden), m2, rm2) * nd;
     }
   }
   if (active) partial[((int64_t)p * S + s) * np + j] = sum;
