@@ -679,6 +679,53 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+PROFILE_CASES = ("flux_mixed_cfg1", "flux_fp64_cfg1", "pd_fp64_51x51", "spectrum_mixed_3a256", "shoot_cfg1")
+
+
+def run_case(name):
+    """One small workload, run twice, for an ncu capture of its kernel (no timing, no JSON line):
+    flux_mixed_cfg1 / flux_fp64_cfg1: the config-1 map at 3*E1 (mixed / plain FP64); pd_fp64_51x51:
+    config 2's power density on 51 x 51 points (40001-point trajectory, plain FP64);
+    spectrum_mixed_3a256: 256 electrons of config 3a's shape (20001 points, 2000 energies, mixed);
+    shoot_cfg1: the config-1 trajectory integrated parallel in time."""
+    import numpy as np
+    import torch
+
+    from srsoriginal_b200 import _lib, device as D, workloads as W
+    from srsoriginal_b200.sr import energy_grid, rectangle_points
+    part, _ = D.ideal_particle(W.ENERGY_GEV, [0, 0, -1], [0, 0, 1])
+    und = [D.undulator([0, W.BPEAK, 0], [0, 0, W.PERIOD], W.NPERIODS)]
+    charge, current = -D.QE, W.CURRENT
+    for _ in range(2):
+        if name in ("flux_mixed_cfg1", "flux_fp64_cfg1"):
+            tr = D.trajectory(und, [part], 0.0, 2.0, 0.0, NT)
+            xyz, _, _, grid = rectangle_points([GRID_N, GRID_N], "XY", [WIDTH, WIDTH], translation=[0, 0, W.SCREEN_Z])
+            out = torch.empty(GRID_N * GRID_N, dtype=torch.float64, device="cuda")
+            if name == "flux_mixed_cfg1":
+                D.flux(tr, charge, current, W.E3_EV, out, grid=grid, precision=_lib.MIXED)
+            else:
+                pts = torch.as_tensor(np.ascontiguousarray(xyz.reshape(-1)), device="cuda")
+                D.flux(tr, charge, current, W.E3_EV, out, points=pts, precision=_lib.FP64)
+        elif name == "pd_fp64_51x51":
+            epu = und + [D.undulator([0.6, 0, 0], [0, 0, W.PERIOD], W.NPERIODS, phase=np.pi / 2)]
+            t2 = D.trajectory(epu, [part], 0.0, 2.0, 0.0, 40001)
+            xyz, _, nrm, _ = rectangle_points([51, 51], "XY", [0.04, 0.04], translation=[0, 0, W.SCREEN_Z])
+            pts = torch.as_tensor(np.ascontiguousarray(xyz.reshape(-1)), device="cuda")
+            nrms = torch.as_tensor(np.ascontiguousarray(np.tile(nrm, (51 * 51, 1)).reshape(-1)), device="cuda")
+            out = torch.empty(51 * 51, dtype=torch.float64, device="cuda")
+            D.power_density(t2, charge, current, out, points=pts, normals=nrms, precision=_lib.FP64)
+        elif name == "spectrum_mixed_3a256":
+            tb = D.trajectory(und, [part] * 256, 0.0, 2.0, 0.0, NT)
+            e = torch.tensor(energy_grid(2000, 100.0, 1000.0), dtype=torch.float64, device="cuda")
+            out = torch.empty(256 * 2000, dtype=torch.float64, device="cuda")
+            D.spectrum(tb, charge, current, [0, 0, W.SCREEN_Z], e, out, precision=_lib.MIXED)
+        elif name == "shoot_cfg1":
+            D.trajectory_shoot(und, part, 0.0, 2.0, 0.0, NT)
+        torch.cuda.synchronize()
+    log(f"case {name} ok")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -689,7 +736,11 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
     ap.add_argument("--cpu-baselines", action="store_true",
                     help="time the reference's CPU path on every configuration and exit")
+    ap.add_argument("--case", choices=PROFILE_CASES,
+                    help="run one small workload twice for a profiler capture of its kernel, and exit")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args.case)
     if args.cpu_baselines:  # the reference on every configuration, host only
         print(json.dumps(cpu_baselines_all()), flush=True)
         return 0

@@ -48,6 +48,11 @@ const char *srs_version(void);
 /* Number of CUDA devices (OSCARSSR_Cuda_GetDeviceCount, src/OSCARSSR_Cuda.cu:30-36). */
 int srs_device_count(void);
 
+/* The library's temporary device buffers come from its own stream-ordered memory pool on each device,
+ * which keeps freed blocks for the next call (no counterpart in the reference, which allocates host
+ * memory only).  This returns the current device's unused blocks to the driver. */
+srs_status srs_trim_memory(void);
+
 /* ------------------------------------------------------------------ fields */
 
 enum { SRS_FIELD_UNDULATOR = 1, SRS_FIELD_GAUSSIAN = 2, SRS_FIELD_UNIFORM_BOX = 3, SRS_FIELD_GRID = 4 };

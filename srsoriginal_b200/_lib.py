@@ -77,6 +77,7 @@ def _load():
         "srs_last_error": (C.c_char_p, []),
         "srs_version": (C.c_char_p, []),
         "srs_device_count": (C.c_int, []),
+        "srs_trim_memory": (S, []),
         "srs_trajectory_counts": (S, [C.c_double, C.c_double, C.c_double, C.c_int64, _D,
                                       C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "srs_trajectory": (S, [C.POINTER(Field), C.c_int32, C.POINTER(Particle), C.c_int32, C.c_double,
@@ -171,7 +172,7 @@ def _load():
 
 lib = _load()
 EXPORTED = (
-    "srs_last_error srs_version srs_device_count srs_trajectory_counts srs_trajectory srs_trajectory_shoot srs_spectrum "
+    "srs_last_error srs_version srs_device_count srs_trim_memory srs_trajectory_counts srs_trajectory srs_trajectory_shoot srs_spectrum "
     "srs_flux srs_power_density srs_total_power srs_accumulate srs_sim_create srs_sim_destroy "
     "srs_sim_set_ctstartstop srs_sim_set_npoints_trajectory srs_sim_get_ctstartstop "
     "srs_sim_get_npoints_trajectory srs_sim_set_nthreads_global srs_sim_set_gpu_global "

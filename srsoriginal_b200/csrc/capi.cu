@@ -1,6 +1,8 @@
 // C ABI of the kernels (include/srs_b200.h): argument checks, stream-ordered scratch, dispatch.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -24,6 +26,31 @@ srs_status cuda_fail(cudaError_t e, const char *what) {
   return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? SRS_ERR_NO_DEVICE : SRS_ERR_CUDA;
 }
 
+cudaError_t library_pool(cudaMemPool_t *pool) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    e = cudaMemPoolCreate(&p, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = ~0ull;  // keep freed blocks for reuse until srs_trim_memory
+    e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+    pools[dev] = p;
+  }
+  *pool = pools[dev];
+  return cudaSuccess;
+}
+
 static srs_status check_view(const srs_traj_view &t, bool need_aoc) {
   if (!t.x || !t.beta || (need_aoc && !t.aoc)) return fail(SRS_ERR_INVALID, "trajectory pointers are NULL");
   if (t.n < 1) return fail(SRS_ERR_RANGE, "no points in trajectory.  Is particle or beam defined?");
@@ -40,6 +67,14 @@ extern "C" {
 
 const char *srs_last_error(void) { return g_error.c_str(); }
 const char *srs_version(void) { return "srs_b200 1.0.0 (sm_100a)"; }
+
+srs_status srs_trim_memory(void) {
+  clear_error();
+  cudaMemPool_t pool;
+  SRS_CUDA(library_pool(&pool));
+  SRS_CUDA(cudaMemPoolTrimTo(pool, 0));
+  return SRS_OK;
+}
 
 int srs_device_count(void) {
   int n = 0;
