@@ -478,6 +478,9 @@ __device__ __forceinline__ void points_flux_tile(const double *__restrict__ xp, 
 struct SpecShared {
   double tau[kSub];
   float v[10][kSub];
+  // each thread's FP64 sums of its energies, [energy q * 6 + component][thread]: in shared memory rather
+  // than registers (48 of them at four energies), so that more CTAs fit an SM
+  double e[kEnergiesPerThread * 6][kThreads];
 };
 
 // Each thread owns K consecutive energies (kEnergiesPerThread, or 2 for spectra too small to fill
@@ -514,11 +517,9 @@ __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, con
   float2 kap2[K / 2];
 #pragma unroll
   for (int pq = 0; pq < K / 2; ++pq) kap2[pq] = f2(kap[2 * pq], kap[2 * pq + 1]);
-  double E[K][6];
+  double(*E)[kThreads] = sh.e;  // E[q * 6 + c][tid]: only this thread's column
 #pragma unroll
-  for (int q = 0; q < K; ++q)
-#pragma unroll
-    for (int c = 0; c < 6; ++c) E[q][c] = 0;
+  for (int q = 0; q < K * 6; ++q) E[q][tid] = 0;
 
   for (int64_t base = i0; base < iend; base += kSub) {
     const int cnt = (int)imin64(kSub, iend - base);
@@ -606,8 +607,8 @@ __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, con
     for (int pq = 0; pq < K / 2; ++pq)
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        E[2 * pq][c] += (double)acc[pq][c].x;
-        E[2 * pq + 1][c] += (double)acc[pq][c].y;
+        E[(2 * pq) * 6 + c][tid] += (double)acc[pq][c].x;
+        E[(2 * pq + 1) * 6 + c][tid] += (double)acc[pq][c].y;
       }
   }
   if (active) {
@@ -617,7 +618,7 @@ __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, con
       if (k >= ne) break;
       double *o = out6 + k;
 #pragma unroll
-      for (int c = 0; c < 6; ++c) o[c * ne] = E[q][c];
+      for (int c = 0; c < 6; ++c) o[c * ne] = E[q * 6 + c][tid];
     }
   }
 }
