@@ -447,14 +447,24 @@ def measure_configs(dev):
                                   "device_phases_note": "RK4 batch of 4096 ideal particles (the same step count "
                                                         "as the sampled ones) and the mixed sums over it, CUDA events"}
 
-    # config 3b: 256 heterogeneous jobs in one persistent launch (CUDA graph), against the same jobs as
-    # separate one-shot calls
+    # config 3b: 256 heterogeneous jobs, trajectories included.  The queue integrates the jobs'
+    # trajectories itself (grouped by length, each group's RK4 batch followed by its work items on a
+    # branch of one CUDA graph) with the tile shape its autotuner picks on these jobs; against it, the
+    # same work as separate calls: one batched RK4 launch for all 256 trajectories, then one one-shot
+    # mixed call per job.  Also the tuned queue on trajectories integrated beforehand (sums only).
     specs = W.config3b_jobs()
-    q, jobs, trajs = W.build_config3b(specs, chunk=8192, ctas_per_sm=0)
+    t_tune = time.perf_counter()
+    q, jobs, trajs = W.build_config3b(specs, integrate=True, tune=True)
+    tune_s = time.perf_counter() - t_tune
+    shape = {"chunk": q.chunk, "ctas_per_sm": q.ctas_per_sm, "energies_per_thread": q.energies_per_thread,
+             "strip_width": q.strip_width, "groups": q.groups}
     ms = _events_ms(q.run, 5)
+    qs, jobs_s, trajs_s = W.build_config3b(specs, shape=dict(shape, groups=1))
+    ms_sums = _events_ms(qs.run, 5)
 
     def separate():
-        for (j, keep), t_, s_ in zip(jobs, trajs, specs):
+        Q.trajectory_batch(und, [part] * len(specs), 0.0, 2.0, 0.0, [s_["nt"] for s_ in specs])
+        for (j, keep), t_, s_ in zip(jobs_s, trajs_s, specs):
             if s_["kind"] == "flux":
                 D.flux(t_, charge, current, W.E1_EV, keep[-1], grid=j.grid, precision=_lib.MIXED)
             else:
@@ -462,10 +472,15 @@ def measure_configs(dev):
     ms_sep = _events_ms(separate, 3)
     rk = _events_ms(lambda: Q.trajectory_batch(und, [part] * len(specs), 0.0, 2.0, 0.0, [s_["nt"] for s_ in specs]), 2)
     out["cfg3b_queue"] = {"evals": q.evals, "queue_ms": ms, "evals_per_s": q.evals / (ms * 1e-3),
-                          "separate_calls_ms": ms_sep, "queue_speedup": ms_sep / ms, "work_items": q.nitems,
-                          "ctas": q.grid, "chunk": q.chunk, "trajectory_batch_ms": rk}
+                          "includes": "the 256 trajectories (integrated parallel in time, grouped by length) and all sums, one CUDA graph",
+                          "separate_calls_ms": ms_sep, "queue_speedup": ms_sep / ms,
+                          "separate_calls_include": "one batched RK4 launch for all trajectories, then a one-shot "
+                                                    "mixed call per job",
+                          "queue_sums_only_ms": ms_sums, "trajectory_batch_ms": rk,
+                          "work_items": q.nitems, "ctas": q.grid, "shape": shape, "autotune_s": tune_s}
     q.close()
-    del jobs, trajs
+    qs.close()
+    del jobs, trajs, jobs_s, trajs_s
 
     # config 4: adjoint / forward time (forward = RK4 through the 2001-sample grid + mixed spectrum of
     # 200 energies; adjoint = sum adjoint + trajectory adjoint scan, FP64)

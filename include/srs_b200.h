@@ -294,6 +294,30 @@ typedef struct srs_queue srs_queue;
  * spectrum jobs' energies once). */
 srs_status srs_queue_create(srs_queue **out, const srs_job *jobs, int32_t njobs, int32_t chunk,
                             int32_t ctas_per_sm);
+
+/* The tile shape of a queue's work items (the autotuner's search space). */
+typedef struct srs_queue_shape {
+  int32_t chunk;               /* trajectory points per work item (>= 128; rounded up to 128s) */
+  int32_t ctas_per_sm;         /* resident CTAs per SM of the persistent grid (0: as many as fit) */
+  int32_t energies_per_thread; /* spectrum items: 2 or 4 energies per thread (0: 4) */
+  int32_t strip_width;         /* flux items: widest strip of grid points in a tile, 8..16 (0: 16) */
+  int32_t groups;              /* with trajectories: groups of jobs by trajectory length (0: 16) */
+} srs_queue_shape;
+
+/* srs_queue_create with a tile shape and, optionally, the jobs' trajectories integrated inside the
+ * queue's graph (no counterpart in the reference, whose calls each integrate and sum one particle).
+ * particles == NULL: the jobs' trajectories are given, as for srs_queue_create.  Otherwise particle j
+ * (HOST array of njobs) is integrated through the HOST field list (the same fields for every job, at
+ * most 16) with ctstart[j], ctstop[j], t0[j], npoints[j] (as srs_trajectory) into job j's trajectory
+ * view -- its x, beta and aoc arrays must hold exactly that many points -- by every srs_queue_run:
+ * the jobs are split into `groups` groups by trajectory length, and each group is one branch of the
+ * graph: its trajectories integrated parallel in time (as srs_trajectory_shoot: within ~1e-15 m of the
+ * serial RK4, magnetic fields only), then its work items, so the sums of some groups overlap the
+ * integration of the others. */
+srs_status srs_queue_create_shaped(srs_queue **out, const srs_job *jobs, int32_t njobs, const srs_queue_shape *shape,
+                                   const srs_field *fields, int32_t nfields, const srs_particle *particles,
+                                   const double *ctstart, const double *ctstop, const double *t0,
+                                   const int64_t *npoints);
 /* Run every job once, ordered after the work already queued on stream; later work on stream waits
  * for the results. */
 srs_status srs_queue_run(srs_queue *q, void *stream);

@@ -54,6 +54,11 @@ class Job(C.Structure):
 JOB_FLUX, JOB_SPECTRUM = 0, 1
 
 
+class QueueShape(C.Structure):
+    _fields_ = [("chunk", C.c_int32), ("ctas_per_sm", C.c_int32), ("energies_per_thread", C.c_int32),
+                ("strip_width", C.c_int32), ("groups", C.c_int32)]
+
+
 class BeamArgs(C.Structure):
     _fields_ = [("type", C.c_char_p), ("name", C.c_char_p), ("energy_gev", C.c_double), ("d0", _V3),
                 ("x0", _V3), ("sigma_energy_gev", C.c_double), ("t0", C.c_double),
@@ -144,6 +149,9 @@ def _load():
         "srs_measure_peak": (S, [C.c_int32, _D, P]),
         "srs_flux_mixed_noalloc": (S, [TrajView, BeamConsts, C.POINTER(Grid2D), C.c_double, P, P]),
         "srs_queue_create": (S, [C.POINTER(P), C.POINTER(Job), C.c_int32, C.c_int32, C.c_int32]),
+        "srs_queue_create_shaped": (S, [C.POINTER(P), C.POINTER(Job), C.c_int32, C.POINTER(QueueShape),
+                                        C.POINTER(Field), C.c_int32, C.POINTER(Particle), _D, _D, _D,
+                                        C.POINTER(C.c_int64)]),
         "srs_queue_run": (S, [P, P]),
         "srs_queue_info": (S, [P, C.POINTER(C.c_int64), _D, C.POINTER(C.c_size_t), C.POINTER(C.c_int32)]),
         "srs_queue_destroy": (None, [P]),
@@ -185,7 +193,7 @@ EXPORTED = (
     "srs_sim_calculate_trajectory srs_sim_calculate_spectrum srs_sim_calculate_flux srs_sim_calculate_flux_plane "
     "srs_sim_calculate_power_density srs_sim_calculate_total_power srs_energy_grid "
     "srs_rectangle_plane srs_rectangle_points srs_measure_peak srs_flux_mixed_noalloc "
-    "srs_queue_create srs_queue_run srs_queue_info srs_queue_destroy srs_trajectory_batch "
+    "srs_queue_create srs_queue_create_shaped srs_queue_run srs_queue_info srs_queue_destroy srs_trajectory_batch "
     "srs_spectrum_efield srs_spectrum_adjoint srs_trajectory_adjoint srs_spectrum_host srs_flux_host "
     "srs_power_density_host"
 ).split()

@@ -90,9 +90,11 @@ struct StripTiles {
 // Points of one tile of a strip w points wide: kThreads, or 16 rows of a narrower strip.
 __host__ __device__ inline int strip_tile_points(int w) { return 16 * w < kThreads ? 16 * w : kThreads; }
 
-inline StripTiles strip_tiles(int n1, int n2) {
+// wmax (8..16): the widest strip allowed (a tunable of the job queue; 16 elsewhere).
+inline StripTiles strip_tiles(int n1, int n2, int wmax = 16) {
   StripTiles best{};
-  const int lo = std::max(1, (n2 + 15) / 16), hi = std::max(lo, n2 / 8);
+  wmax = std::min(16, std::max(8, wmax));
+  const int lo = std::max(1, (n2 + wmax - 1) / wmax), hi = std::max(lo, n2 / 8);
   for (int ns = lo; ns <= hi; ++ns) {
     StripTiles m{};
     m.n1 = n1;
@@ -110,7 +112,7 @@ inline StripTiles strip_tiles(int n1, int n2) {
   }
   return best;
 }
-inline StripTiles strip_tiles(const srs_grid2d &g) { return strip_tiles(g.n1, g.n2); }
+inline StripTiles strip_tiles(const srs_grid2d &g, int wmax = 16) { return strip_tiles(g.n1, g.n2, wmax); }
 
 // Thread tid's grid point (i1, i2) in tile `tile`, whether it holds one, the tile's anchor point
 // (ca, cb): the middle row of the tile's points and the middle column of its strip, and the largest

@@ -105,12 +105,15 @@ def config3b_jobs(n=256, seed=3):
     return jobs
 
 
-def build_config3b(specs, chunk=None, ctas_per_sm=0, tune=False):
+def build_config3b(specs, chunk=None, ctas_per_sm=0, tune=False, integrate=False, shape=None):
     """Device jobs of a config-3b style spec list (from :func:`config3b_jobs`): the ideal 3 GeV
-    particle through the config-0 undulator, each job with its own trajectory length (all computed
-    by one srs_trajectory_batch launch), flux maps on a 10 mm square at 30 m at E1, spectra on axis
-    at 30 m over the reference's 100-1000 eV energy grid.  Returns (JobQueue, jobs, trajectories);
-    job outputs are jobs[i][1][-1].  tune: pick (chunk, CTAs per SM) with queue.autotune."""
+    particle through the config-0 undulator, each job with its own trajectory length, flux maps on a
+    10 mm square at 30 m at E1, spectra on axis at 30 m over the reference's 100-1000 eV energy grid.
+    Returns (JobQueue, jobs, trajectories); job outputs are jobs[i][1][-1].  integrate: the queue
+    integrates the trajectories itself on every run (grouped by length, overlapped with the sums);
+    otherwise one srs_trajectory_batch launch computes them here.  shape: JobQueue keyword arguments
+    (chunk, ctas_per_sm, energies_per_thread, strip_width, groups); tune: pick them with
+    queue.autotune."""
     import torch
 
     from . import device as D
@@ -119,7 +122,13 @@ def build_config3b(specs, chunk=None, ctas_per_sm=0, tune=False):
 
     und = D.undulator([0, BPEAK, 0], [0, 0, PERIOD], NPERIODS)
     part, _ = D.ideal_particle(ENERGY_GEV, [0, 0, -1], [0, 0, 1])
-    trajs = Q.trajectory_batch([und], [part] * len(specs), 0.0, 2.0, 0.0, [s["nt"] for s in specs])
+    nts = [s["nt"] for s in specs]
+    if integrate:
+        trajs = Q.trajectory_buffers([0.0] * len(specs), [2.0] * len(specs), [0.0] * len(specs), nts)
+        how = dict(fields=[und], particles=[part] * len(specs), ctstart=0.0, ctstop=2.0, t0=0.0, npoints=nts)
+    else:
+        trajs = Q.trajectory_batch([und], [part] * len(specs), 0.0, 2.0, 0.0, nts)
+        how = None
     charge, current = -D.QE, CURRENT
     jobs, grids, energies = [], {}, {}
     for s, t in zip(specs, trajs):
@@ -135,9 +144,15 @@ def build_config3b(specs, chunk=None, ctas_per_sm=0, tune=False):
                 energies[ne] = torch.tensor(energy_grid(ne, 100.0, 1000.0), dtype=torch.float64, device="cuda")
             out = torch.empty(ne, dtype=torch.float64, device="cuda")
             jobs.append(Q.spectrum_job(t, charge, current, [0, 0, SCREEN_Z], energies[ne], out))
+    sh = dict(shape or {})
+    if chunk is not None:
+        sh["chunk"] = chunk
+    if ctas_per_sm:
+        sh["ctas_per_sm"] = ctas_per_sm
     if tune:
-        chunk, ctas_per_sm, _ = Q.autotune(jobs)
-    q = Q.JobQueue(jobs, chunk or 2048, ctas_per_sm)
+        sh, _ = Q.autotune(jobs, integrate=how)
+    sh.setdefault("chunk", 2048)
+    q = Q.JobQueue(jobs, integrate=how, **sh)
     return q, jobs, trajs
 
 

@@ -102,12 +102,45 @@ def test_autotune_caches(tmp_path, monkeypatch, small_specs):
     from srsoriginal_b200 import queue as Q, workloads as W
     monkeypatch.setenv("SRS_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     q, jobs, _ = W.build_config3b(small_specs[:3])
-    ch, c, table = Q.autotune(jobs, chunks=(1024, 4096), ctas_per_sm=(1, 0), reps=1)
-    assert (ch, c) in table and len(table) == 4
+    best, table = Q.autotune(jobs, chunks=(1024, 4096), ctas_per_sm=(0,), energies_per_thread=(2, 4),
+                             strip_widths=(8, 16), reps=1)
+    assert len(table) == 8 and tuple(sorted(best.items())) in table
     assert (tmp_path / "tune.json").exists()
-    ch2, c2, table2 = Q.autotune(jobs, chunks=(1024, 4096), ctas_per_sm=(1, 0), reps=1)
-    assert (ch2, c2) == (ch, c) and table2 == {}
+    best2, table2 = Q.autotune(jobs, chunks=(1024, 4096), ctas_per_sm=(0,), energies_per_thread=(2, 4),
+                               strip_widths=(8, 16), reps=1)
+    assert best2 == best and table2 == {}
     q.close()
+
+
+@pytest.mark.parametrize("shape", [dict(chunk=1024, energies_per_thread=2, strip_width=8, groups=3),
+                                   dict(chunk=4096, energies_per_thread=4, strip_width=16, groups=1)])
+def test_queue_integrating_trajectories_matches_given_trajectories(small_specs, shape):
+    """A queue that integrates its jobs' trajectories (grouped by length, each group's trajectories
+    integrated parallel in time and then its items, one branch of the graph per group) against the
+    same queue shape on trajectories integrated beforehand by the serial RK4: the trajectories within
+    the parallel-in-time tolerances (positions 2e-14 m, beta 2e-14, a/c 1e-12 of its largest value),
+    the outputs within 1e-6; and the same again on a replay of the graph."""
+    from srsoriginal_b200 import workloads as W
+    q0, jobs0, trajs0 = W.build_config3b(small_specs, shape=shape)
+    q1, jobs1, trajs1 = W.build_config3b(small_specs, shape=shape, integrate=True)
+    q0.run()
+
+    def check():
+        q1.run()
+        torch.cuda.synchronize()
+        for t0, t1 in zip(trajs0, trajs1):
+            assert float((t0.x - t1.x).abs().max()) <= 2e-14
+            assert float((t0.beta - t1.beta).abs().max()) <= 2e-14
+            assert float((t0.aoc - t1.aoc).abs().max()) <= 1e-12 * float(t0.aoc.abs().max())
+        for (_, k0), (_, k1) in zip(jobs0, jobs1):
+            assert _rel(k1[-1].cpu().numpy(), k0[-1].cpu().numpy()) <= 1e-6
+
+    check()
+    for t in trajs1:
+        t.x.fill_(0.0)  # the next run must integrate them again
+    check()
+    q0.close()
+    q1.close()
 
 
 def test_queue_rejects_bad_jobs():
