@@ -457,9 +457,9 @@ def measure_configs(dev):
     q, jobs, trajs = W.build_config3b(specs, integrate=True, tune=True)
     tune_s = time.perf_counter() - t_tune
     shape = {"chunk": q.chunk, "ctas_per_sm": q.ctas_per_sm, "energies_per_thread": q.energies_per_thread,
-             "strip_width": q.strip_width, "groups": q.groups}
+             "strip_width": q.strip_width, "groups": q.groups, "steps_per_segment": q.steps_per_segment}
     ms = _events_ms(q.run, 5)
-    qs, jobs_s, trajs_s = W.build_config3b(specs, shape=dict(shape, groups=1))
+    qs, jobs_s, trajs_s = W.build_config3b(specs, shape=dict(shape, groups=1, steps_per_segment=0))
     ms_sums = _events_ms(qs.run, 5)
 
     def separate():

@@ -302,6 +302,9 @@ typedef struct srs_queue_shape {
   int32_t energies_per_thread; /* spectrum items: 2 or 4 energies per thread (0: 4) */
   int32_t strip_width;         /* flux items: widest strip of grid points in a tile, 8..16 (0: 16) */
   int32_t groups;              /* with trajectories: groups of jobs by trajectory length (0: 16) */
+  int32_t steps_per_segment;   /* with trajectories: RK4 steps per segment of the parallel-in-time
+                                  integrations (0: 16; longer segments use less shared memory, so more
+                                  integrations run side by side) */
 } srs_queue_shape;
 
 /* srs_queue_create with a tile shape and, optionally, the jobs' trajectories integrated inside the

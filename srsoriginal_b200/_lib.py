@@ -56,7 +56,7 @@ JOB_FLUX, JOB_SPECTRUM = 0, 1
 
 class QueueShape(C.Structure):
     _fields_ = [("chunk", C.c_int32), ("ctas_per_sm", C.c_int32), ("energies_per_thread", C.c_int32),
-                ("strip_width", C.c_int32), ("groups", C.c_int32)]
+                ("strip_width", C.c_int32), ("groups", C.c_int32), ("steps_per_segment", C.c_int32)]
 
 
 class BeamArgs(C.Structure):

@@ -132,7 +132,7 @@ struct srs_queue {
   int64_t *d_offsets = nullptr;
   unsigned int *d_ticket = nullptr;  // one per group
   double *d_scratch = nullptr;       // partials, then the spectrum jobs' angular frequencies
-  int njobs = 0, nitems = 0, grid = 0, K = kEnergiesPerThread, per_sm = 1, sms = 148;
+  int njobs = 0, nitems = 0, grid = 0, K = kEnergiesPerThread, per_sm = 1, sms = 148, seg_steps = 16;
   int64_t total_out = 0;
   double evals = 0;
   size_t scratch_bytes = 0;
@@ -199,10 +199,13 @@ srs_status srs_queue_create_shaped(srs_queue **out, const srs_job *jobs, int32_t
   if (integrate && nfields > kRk4MaxFields)
     return fail(SRS_ERR_RANGE, "trajectories: at most " + std::to_string(kRk4MaxFields) + " fields");
   int groups = integrate ? (shape->groups == 0 ? 16 : shape->groups) : 1;
+  const int seg_steps = shape->steps_per_segment == 0 ? 16 : shape->steps_per_segment;
+  if (seg_steps < 1) return fail(SRS_ERR_INVALID, "steps_per_segment must be >= 1 (or 0)");
   if (groups < 1) return fail(SRS_ERR_INVALID, "groups must be >= 1");
   groups = std::min(groups, (int)njobs);
   std::unique_ptr<srs_queue> q(new srs_queue());
   q->K = K;
+  q->seg_steps = seg_steps;
   std::vector<QJob> hj(njobs);
   std::vector<int64_t> offsets(njobs + 1, 0);
   // group of each job: by trajectory length (shortest first), equal numbers of jobs per group
@@ -332,7 +335,7 @@ srs_status srs_queue_create_shaped(srs_queue **out, const srs_job *jobs, int32_t
                                                 const_cast<double *>(jobs[j].traj.beta),
                                                 const_cast<double *>(jobs[j].traj.aoc)});
         hp.push_back(particles[j]);
-        need = std::max(need, shoot_scratch_bytes(nf, nb, 0, nfields));
+        need = std::max(need, shoot_scratch_bytes(nf, nb, seg_steps, nfields));
       }
       if (need > 0) SRS_CUDA(cudaMalloc(&q->shoot_scratch[g], need));
     }
@@ -366,7 +369,7 @@ srs_status srs_queue_create_shaped(srs_queue **out, const srs_job *jobs, int32_t
 
 srs_status srs_queue_create(srs_queue **out, const srs_job *jobs, int32_t njobs, int32_t chunk,
                             int32_t ctas_per_sm) {
-  const srs_queue_shape shape{chunk, ctas_per_sm, 0, 0, 1};
+  const srs_queue_shape shape{chunk, ctas_per_sm, 0, 0, 1, 0};
   return srs_queue_create_shaped(out, jobs, njobs, &shape, nullptr, 0, nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 
@@ -389,7 +392,7 @@ srs_status srs_queue_run(srs_queue *q, void *stream) {
         for (const srs_queue::Shoot &t : q->shoots[g]) {
           if (launch != cudaSuccess) break;
           launch = launch_rk4_shoot(q->d_fields, q->nfields, q->d_particles + t.index, t.host, t.dt, t.nf, t.nb, t.x,
-                                    t.b, t.a, a, q->stage, 0, 0, q->shoot_scratch[g], nullptr);
+                                    t.b, t.a, a, q->stage, q->seg_steps, 0, q->shoot_scratch[g], nullptr);
         }
       const int n_g = q->gofs[g + 1] - q->gofs[g];
       if (launch == cudaSuccess && n_g > 0) {

@@ -49,6 +49,7 @@ constexpr double kTol = 4.440892098500626e-16;  // 2^-51 (~2 ulps of the speed):
 constexpr double kNear = 9.5367431640625e-07;   // 2^-20: keep the Jacobians, store the points
 constexpr int kChunkDoubles = 132;               // per-chunk data staged for the sweep
 constexpr int kMaxChunks = 192;                  // 192 x 132 doubles = 198 KB of shared memory
+constexpr int kOneWaveChunks = 148;              // the B200's SMs: one pass block (chunk) per SM
 
 struct Plan {
   int64_t mf, mb;         // steps of each chain
@@ -487,8 +488,21 @@ Plan make_plan(int64_t nfwd, int64_t nbwd, double dt, int steps_per_segment, int
   Plan P;
   P.mf = nfwd > 0 ? nfwd - 1 : 0;
   P.mb = nbwd;
-  P.L = steps_per_segment > 0 ? steps_per_segment : shoot_default_steps(P.mf + P.mb);
   P.m = kShootThreads / lanes_for(nfields);
+  auto chunks_for = [&](int64_t L) {
+    return ((P.mf + L - 1) / L + P.m - 1) / P.m + ((P.mb + L - 1) / L + P.m - 1) / P.m;
+  };
+  if (steps_per_segment > 0) {
+    P.L = steps_per_segment;
+  } else {
+    // A pass costs ~0.9 us per step of a segment (the blocks integrate their segments side by side)
+    // plus ~0.09 us per chunk (the sequential sweep): L = sqrt(steps / 160) balances the two.  A pass
+    // runs one block per chunk, one per SM (the sweep's shared memory), so longer segments when the
+    // chunks would not fit one wave of kOneWaveChunks.
+    int64_t L = shoot_default_steps(P.mf + P.mb);
+    while (chunks_for(L) > kOneWaveChunks) ++L;
+    P.L = (int)L;
+  }
   // at most kMaxChunks chunks (their data are staged in shared memory for the sweep): longer segments
   // than asked for if needed
   while (((P.mf + P.L - 1) / P.L + (P.mb + P.L - 1) / P.L) > (int64_t)(kMaxChunks - 2) * P.m) P.L *= 2;
@@ -553,11 +567,11 @@ cudaError_t launch_pass_g(int G, int blocks, size_t smem, cudaStream_t s, const 
 }  // namespace
 
 int shoot_default_steps(int64_t nsteps) {
-  // 16 steps per segment: each iteration costs ~16 serial steps plus a chunk sweep; long
-  // trajectories keep the segment count near 4096
-  int64_t L = 16;
-  while (L * 4096 < nsteps && L < 4096) L *= 2;
-  return (int)L;
+  // steps per segment that balance a pass's integration (~0.9 us per step) against its sequential
+  // chunk sweep (~0.09 us per chunk of 16 segments): L = sqrt(steps / 160), at least 4 (measured on
+  // B200: 5001 to 40001 points, 14-25 % faster than 16 steps throughout)
+  const int64_t L = llround(sqrt((double)std::max<int64_t>(nsteps, 1) / 160.0));
+  return (int)std::max<int64_t>(4, L);
 }
 
 size_t shoot_scratch_bytes(int64_t nfwd, int64_t nbwd, int steps_per_segment, int nfields) {

@@ -31,6 +31,7 @@ CTAS_PER_SM = (0,)  # 0: as many as fit
 ENERGIES_PER_THREAD = (2, 4)
 STRIP_WIDTHS = (8, 12, 16)
 GROUPS = (8, 4, 16, 32)
+SEGMENT_STEPS = (16, 32)  # steps per segment of the queue's parallel-in-time integrations
 
 
 def flux_job(traj, charge, current, grid, energy_ev, out):
@@ -63,14 +64,15 @@ class JobQueue:
     """The planned queue of a list of jobs (from :func:`flux_job` / :func:`spectrum_job`)."""
 
     def __init__(self, jobs, chunk=2048, ctas_per_sm=0, energies_per_thread=0, strip_width=0, integrate=None,
-                 groups=0):
+                 groups=0, steps_per_segment=0):
         """integrate: None (the jobs' trajectories are given), or a dict (fields, particles, ctstart,
         ctstop, t0, npoints; per-job sequences except fields) with which every run integrates them into
         the jobs' trajectory views (see :func:`trajectory_buffers`) in ``groups`` length groups."""
         self._keep = [k for _, k in jobs]  # the tensors must outlive the queue
         arr = (_lib.Job * len(jobs))(*[j for j, _ in jobs])
         self._q = C.c_void_p()
-        shape = _lib.QueueShape(int(chunk), int(ctas_per_sm), int(energies_per_thread), int(strip_width), int(groups))
+        shape = _lib.QueueShape(int(chunk), int(ctas_per_sm), int(energies_per_thread), int(strip_width), int(groups),
+                                int(steps_per_segment))
         if integrate is None:
             check(lib.srs_queue_create_shaped(C.byref(self._q), arr, len(jobs), C.byref(shape), None, 0, None, None,
                                               None, None, None))
@@ -89,6 +91,7 @@ class JobQueue:
                                               vals[2].ctypes.data_as(D), npts.ctypes.data_as(C.POINTER(C.c_int64))))
         self.chunk, self.ctas_per_sm = int(chunk), int(ctas_per_sm)
         self.energies_per_thread, self.strip_width, self.groups = int(energies_per_thread), int(strip_width), int(groups)
+        self.steps_per_segment = int(steps_per_segment)
         self.integrates = integrate is not None
         n, ev, sb, g = C.c_int64(), C.c_double(), C.c_size_t(), C.c_int32()
         check(lib.srs_queue_info(self._q, C.byref(n), C.byref(ev), C.byref(sb), C.byref(g)))
@@ -178,7 +181,7 @@ def autotune(jobs, chunks=CHUNKS, ctas_per_sm=CTAS_PER_SM, energies_per_thread=E
              strip_widths=STRIP_WIDTHS, groups=GROUPS, integrate=None, reps=3, cache=True):
     """Pick the queue's tile shape for this job list by timing candidate queues on the jobs
     themselves: every (chunk, CTAs per SM, energies per thread, strip width), then, with integrate, the
-    number of trajectory-length groups for the best of those.  Returns (shape dict, table) with table
+    number of trajectory-length groups and the integrations' steps per segment for the best of those.  Returns (shape dict, table) with table
     = {shape tuple: ms}.  With cache, a previous result for the same signature is returned without
     timing, and new results are stored."""
     key = signature(jobs) + (":integrate" if integrate is not None else "")
@@ -201,7 +204,7 @@ def autotune(jobs, chunks=CHUNKS, ctas_per_sm=CTAS_PER_SM, energies_per_thread=E
         table[tuple(sorted(sh.items()))] = ms
         return ms
 
-    base = {"groups": groups[0] if integrate is not None else 0}
+    base = {"groups": groups[0], "steps_per_segment": SEGMENT_STEPS[0]} if integrate is not None else {"groups": 0}
     best, best_ms = None, float("inf")
     for ch in chunks:
         for c in ctas_per_sm:
@@ -212,11 +215,15 @@ def autotune(jobs, chunks=CHUNKS, ctas_per_sm=CTAS_PER_SM, energies_per_thread=E
                     if ms < best_ms:
                         best, best_ms = sh, ms
     if integrate is not None:
-        for gr in groups[1:]:
-            sh = dict(best, groups=gr)
-            ms = timed(**sh)
-            if ms < best_ms:
-                best, best_ms = sh, ms
+        start = dict(best)
+        for gr in groups:
+            for L in SEGMENT_STEPS:
+                sh = dict(start, groups=gr, steps_per_segment=L)
+                if sh == start:
+                    continue
+                ms = timed(**sh)
+                if ms < best_ms:
+                    best, best_ms = sh, ms
     if cache:
         db[key] = {"shape": best, "ms": best_ms}
         try:
