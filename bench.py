@@ -331,7 +331,7 @@ def _events_ms(fn, reps, warmup=1):
     return statistics.median(times)
 
 
-def measure_configs(dev):
+def measure_configs(dev, peaks=None):
     """The other configurations' throughput, for the record (not the headline): each device-timed
     with CUDA events (median of a few runs) unless marked wall-clock."""
     import numpy as np
@@ -444,6 +444,9 @@ def measure_configs(dev):
                                   "includes": "public API call: sampling, 4096 RK4, mixed sums, accumulation",
                                   "rk4_batch_ms": rk_ms, "spectrum_sums_ms": sum_ms,
                                   "spectrum_sums_evals_per_s": ev / (sum_ms * 1e-3),
+                                  "spectrum_sums_fp32_frac_of_measured_peak": (
+                                      _COUNTS["spectrum_uniform_mixed"]["fp32"] * ev / (sum_ms * 1e-3)
+                                      / peaks["fp32"] if peaks else None),
                                   "device_phases_note": "RK4 batch of 4096 ideal particles (the same step count "
                                                         "as the sampled ones) and the mixed sums over it, CUDA events"}
 
@@ -682,7 +685,7 @@ def run_ours(args, world, rank, local):
             "roofline": roofline, "clocks": clk, "e2e": e2e, "e2e_fp64": e2e_fp64,
             "gpu_launches": args.steps * len(ENERGIES) * 2}
     if not args.no_configs:
-        line["other_configs"] = measure_configs(dev)
+        line["other_configs"] = measure_configs(dev, peaks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline()

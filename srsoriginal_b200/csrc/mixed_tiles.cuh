@@ -477,19 +477,47 @@ __device__ __forceinline__ void points_flux_tile(const double *__restrict__ xp, 
   }
 }
 
+// Per trajectory point of a spectrum sub-tile, FP32 records whose signs are chosen so that the inner
+// loops need no negation (a = (beta - n)/D, b = n/D^2; rot = exp(i dw tau), rot2 = exp(2 i dw tau)):
+//   p0 = (a_x, a_y, a_z, b_z)     p1 = (-a_x, -a_y, -a_z, -Im rot)
+//   p2 = (rot, rot2) as (re, im, re, im)     p3 = (-Im rot2, b_x, b_y, 0)
 struct SpecShared {
   double tau[kSub];
-  float v[10][kSub];
+  float4 p0[kSub], p1[kSub], p2[kSub], p3[kSub];
+  float red[2][kThreads / 32];  // per-warp sums of the near-field bound of the current sub-tile
+  float wmin[kThreads / 32];    // per-warp smallest angular frequency of the tile's energies
   // each thread's FP64 sums of its energies, [energy q * 6 + component][thread]: in shared memory rather
   // than registers (48 of them at four energies), so that more CTAs fit an SM
   double e[kEnergiesPerThread * 6][kThreads];
 };
 
+// The x and y near-field terms i kap b_perp of a sub-tile are left out when their sum can reach at most
+// kNearPerp times the sub-tile's sum of |a| (kap = -c/w, |kap| largest at the tile's lowest energy).
+// Over a trajectory the terms left out then add up to at most kNearPerp * sum |a|, below the FP32
+// rounding of the sums themselves (~2^-24 sum |a| / sqrt(points) for random rounding, and the output
+// |E| is a fraction of sum |a|).  At 30 m the ratio is ~1e-14 inside an undulator and lambda/(2 pi D)
+// ~ 1e-11 in the drifts; observers a few metres away at low energies keep them.
+constexpr float kNearPerp = 1e-10f;
+
+// x modulo 2 pi for the spectrum's per-(point, thread) phase: the Cody-Waite steps of reduce_2pi
+// without its third part, whose product k * P3 is below 1e-20 rad for |x| < 1e13 rad (phases here are
+// at most ~1e12 rad), so the result equals reduce_2pi's to within an ulp of pi.
+__device__ __forceinline__ double reduce_2pi_short(double x) {
+  const double kInv2Pi = 0.15915494309189535;
+  const double P1 = 6.283185307179586, P2 = 2.4492935982947064e-16;
+  const double k = rint(x * kInv2Pi);
+  return __fma_rn(-k, P2, __fma_rn(-k, P1, x));
+}
+
 // Each thread owns K consecutive energies (kEnergiesPerThread, or 2 for spectra too small to fill
-// the GPU otherwise).  The rotation exp(i dw tau_i) is shared by
-// all threads (dw = (w_last - w_first)/(ne - 1), computed once per trajectory point per CTA); a thread
-// whose energies are not on that uniform grid (|w_k - (w_0 + k dw)| * tau_max > 1e-3 rad) takes one
-// reduced sincos per (point, energy) instead.  No host synchronisation is needed to decide.
+// the GPU otherwise).  On a uniform energy grid the phasors exp(i w_k tau) of a thread's energies are
+// one reduced sincos per (trajectory point, thread) walked by the rotations exp(i dw tau) and
+// exp(2 i dw tau) (dw = (w_last - w_first)/(ne - 1), formed in FP64 once per trajectory point per
+// CTA): the walk is re-anchored every K energies.  A thread whose energies are not on that grid
+// (|w_k - (w_0 + k dw)| * tau_max > 1e-3 rad) takes one reduced sincos per (point, energy) instead.
+// No host synchronisation is needed to decide.  K = 4 is the measured optimum of the walk length: the
+// kernel is bound by the FMA pipe, and every energy walked costs a complex multiply on it, while the
+// sincos it replaces runs on the XU and FP64 pipes.
 // One tile: energies of tile `etile` (kThreads * K of them, K per thread) against trajectory points
 // [i0, iend); writes the six partial sums of every energy to out6[c * ne + k].
 template <int K>
@@ -497,25 +525,30 @@ __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, con
                                               int64_t n, double dt, V3 obs, const double *__restrict__ omegas,
                                               int64_t ne, int etile, int64_t i0, int64_t iend,
                                               double *__restrict__ out6, SpecShared &sh) {
-  double *stau = sh.tau;
-  float (*sv)[kSub] = sh.v;  // a = (beta - n)/D (3), b' = n/D^2 (3), exp(i dw tau) (2), exp(2 i dw tau) (2)
-  const int tid = threadIdx.x;
+  static_assert(K == 2 || K == 4, "energies per thread: 2 or 4");
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t k0 = ((int64_t)etile * kThreads + tid) * K;
   const bool active = k0 < ne;
   const double wfirst = omegas[0];
   const double dw = ne > 1 ? (omegas[ne - 1] - wfirst) / (double)(ne - 1) : 0.0;
   float kap[K];  // -c/w_k: the near-field term is i*kap*n/D^2
-  double wk[K];
+  double wkn[K];  // -w_k: sincos of the negated phase gives (cos, -sin) directly
   bool uniform = ne > 1;
+  float wmin = 3.0e38f;
 #pragma unroll
   for (int q = 0; q < K; ++q) {
     const int64_t k = imin64(k0 + q, ne - 1);
-    wk[q] = omegas[k];
-    kap[q] = (float)(-kC / wk[q]);
-    const double dev = fabs(wk[q] - (wfirst + (double)k * dw));
-    if (k0 + q < ne && dev * (1e3 / kC) >= 1e-3) uniform = false;  // observers within 1 km
+    const double w = omegas[k];
+    wkn[q] = -w;
+    kap[q] = (float)(-kC / w);
+    const double dev = fabs(w - (wfirst + (double)k * dw));
+    if (k0 + q < ne) {
+      if (dev * (1e3 / kC) >= 1e-3) uniform = false;  // observers within 1 km
+      wmin = fminf(wmin, (float)w);
+    }
   }
-  static_assert(K % 2 == 0, "energies per thread come in pairs");
+#pragma unroll
+  for (int o = 16; o; o >>= 1) wmin = fminf(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
   float2 kap2[K / 2];
 #pragma unroll
   for (int pq = 0; pq < K / 2; ++pq) kap2[pq] = f2(kap[2 * pq], kap[2 * pq + 1]);
@@ -523,86 +556,147 @@ __device__ __forceinline__ void spectrum_tile(const double *__restrict__ xp, con
 #pragma unroll
   for (int q = 0; q < K * 6; ++q) E[q][tid] = 0;
 
+  // whether every energy of the CTA is on the uniform grid: the fast loop below then has no branch
+  const bool all_uniform = __syncthreads_and(uniform || !active);
   for (int64_t base = i0; base < iend; base += kSub) {
     const int cnt = (int)imin64(kSub, iend - base);
-    __syncthreads();
+    __syncthreads();  // every thread is done with the previous sub-tile's records and sums
+    float bsum = 0.f, asum = 0.f;
     if (tid < cnt) {
       const int64_t i = base + tid;
       const double rx = obs.x - xp[i], ry = obs.y - xp[n + i], rz = obs.z - xp[2 * n + i];
       const double D = sqrt(rx * rx + ry * ry + rz * rz), iD = 1.0 / D;
       const double nx = rx * iD, ny = ry * iD, nz = rz * iD;
       const double tau = dt * (double)i + D / kC;
-      stau[tid] = tau;
-      sv[0][tid] = (float)((bp[i] - nx) * iD);
-      sv[1][tid] = (float)((bp[n + i] - ny) * iD);
-      sv[2][tid] = (float)((bp[2 * n + i] - nz) * iD);
+      sh.tau[tid] = tau;
+      const float ax = (float)((bp[i] - nx) * iD), ay = (float)((bp[n + i] - ny) * iD),
+                  az = (float)((bp[2 * n + i] - nz) * iD);
       const double iD2 = iD * iD;
-      sv[3][tid] = (float)(nx * iD2);
-      sv[4][tid] = (float)(ny * iD2);
-      sv[5][tid] = (float)(nz * iD2);
+      const float bx = (float)(nx * iD2), by = (float)(ny * iD2), bz = (float)(nz * iD2);
       double sr, cr;
       sincos(reduce_2pi(dw * tau), &sr, &cr);
-      sv[6][tid] = (float)cr;
-      sv[7][tid] = (float)sr;
-      if (K > 2) {
-        sincos(reduce_2pi(2.0 * dw * tau), &sr, &cr);  // the rotation by two energy steps
-        sv[8][tid] = (float)cr;
-        sv[9][tid] = (float)sr;
-      }
+      const float rr = (float)cr, ri = (float)sr;
+      // the rotation by two energy steps, squared in FP64
+      const float r2r = K > 2 ? (float)((cr - sr) * (cr + sr)) : 0.f, r2i = K > 2 ? (float)(2.0 * cr * sr) : 0.f;
+      sh.p0[tid] = make_float4(ax, ay, az, bz);
+      sh.p1[tid] = make_float4(-ax, -ay, -az, -ri);
+      sh.p2[tid] = make_float4(rr, ri, r2r, r2i);
+      sh.p3[tid] = make_float4(-r2i, bx, by, 0.f);
+      bsum = fabsf(bx) + fabsf(by);                          // >= |b_perp|
+      asum = fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az)));  // <= |a|
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
+      asum += __shfl_xor_sync(0xffffffffu, asum, o);
+    }
+    if (lane == 0) {
+      sh.red[0][warp] = bsum;
+      sh.red[1][warp] = asum;
+      sh.wmin[warp] = wmin;
     }
     __syncthreads();
     if (!active) continue;
-    // accumulators packed by energy pairs (q, q+1): acc[p][c] = (e[2p][c], e[2p+1][c])
+    float Bs = 0.f, As = 0.f, wm = 3.0e38f;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+      Bs += sh.red[0][w];
+      As += sh.red[1][w];
+      wm = fminf(wm, sh.wmin[w]);
+    }
+    // the same decision in every thread of the CTA: the same values added in the same order
+    const bool perp_near = (float)kC / wm * Bs > kNearPerp * As;
+    // accumulators packed by energy pairs (q, q+1): acc[p][c] = (e[2p][c], e[2p+1][c]), components
+    // (Re, Im) of E_x, E_y, E_z
     float2 acc[K / 2][6];
 #pragma unroll
     for (int pq = 0; pq < K / 2; ++pq)
 #pragma unroll
       for (int c = 0; c < 6; ++c) acc[pq][c] = f2(0.f, 0.f);
-    for (int k = 0; k < cnt; ++k) {
-      const double tau = stau[k];
-      const float ax = sv[0][k], ay = sv[1][k], az = sv[2][k];
-      const float bx = sv[3][k], by = sv[4][k], bz = sv[5][k];
-      const float rr = sv[6][k], ri = sv[7][k];
-      // z_q = exp(i w_q tau): z_0 from one reduced sincos, then the rotation exp(i dw tau) on a uniform
-      // grid (z_{q+1} = z_q rot for the first pair, the pair times rot^2 for the next), else sincos
-      float2 zr[K / 2], zi[K / 2];
-      float z0r, z0i;
-      __sincosf((float)reduce_2pi(wk[0] * tau), &z0i, &z0r);
-      if (uniform) {
-        const float z1r = z0r * rr - z0i * ri, z1i = fmaf(z0r, ri, z0i * rr);
+
+    // z = exp(i w_q tau) as (zr, zin = -Im z) per energy pair
+    auto phasors = [&](double tau, const float4 &P1, const float4 &P2, const float4 &P3, float2 *zr, float2 *zin,
+                       bool uni) {
+      float z0r, z0n;
+      __sincosf((float)reduce_2pi_short(wkn[0] * tau), &z0n, &z0r);
+      if (uni) {
+        const float rr = P2.x, ri = P2.y, rin = P1.w;
+        const float z1r = fmaf(z0n, ri, z0r * rr), z1n = fmaf(z0r, rin, z0n * rr);
         zr[0] = f2(z0r, z1r);
-        zi[0] = f2(z0i, z1i);
-        const float r2r = sv[8][k], r2i = sv[9][k];  // rot^2
-        const float2 R2r = f2(r2r, r2r), R2i = f2(r2i, r2i);
+        zin[0] = f2(z0n, z1n);
+        const float2 R2r = f2(P2.z, P2.z), R2i = f2(P2.w, P2.w), R2in = f2(P3.x, P3.x);
 #pragma unroll
         for (int pq = 1; pq < K / 2; ++pq) {
-          zr[pq] = fma2(zr[pq - 1], R2r, mul2(neg2(zi[pq - 1]), R2i));
-          zi[pq] = fma2(zr[pq - 1], R2i, mul2(zi[pq - 1], R2r));
+          zr[pq] = fma2(zin[pq - 1], R2i, mul2(zr[pq - 1], R2r));
+          zin[pq] = fma2(zr[pq - 1], R2in, mul2(zin[pq - 1], R2r));
         }
       } else {
-        float cr[K], ci[K];
+        float cr[K], cn[K];
         cr[0] = z0r;
-        ci[0] = z0i;
+        cn[0] = z0n;
 #pragma unroll
-        for (int q = 1; q < K; ++q) __sincosf((float)reduce_2pi(wk[q] * tau), &ci[q], &cr[q]);
+        for (int q = 1; q < K; ++q) __sincosf((float)reduce_2pi_short(wkn[q] * tau), &cn[q], &cr[q]);
 #pragma unroll
         for (int pq = 0; pq < K / 2; ++pq) {
           zr[pq] = f2(cr[2 * pq], cr[2 * pq + 1]);
-          zi[pq] = f2(ci[2 * pq], ci[2 * pq + 1]);
+          zin[pq] = f2(cn[2 * pq], cn[2 * pq + 1]);
         }
       }
-      const float2 Ax = f2(ax, ax), Ay = f2(ay, ay), Az = f2(az, az);
-      const float2 Bx = f2(bx, bx), By = f2(by, by), Bz = f2(bz, bz);
+    };
+
+    if (all_uniform && !perp_near) {
+      // uniform grid, E_x and E_y without their near-field terms; E_z's near-field term summed apart,
+      // sum b_z z, and multiplied by i kap once per sub-tile
+      float2 nzr[K / 2], nzn[K / 2];  // sum b_z Re z, sum b_z (-Im z)
+#pragma unroll
+      for (int pq = 0; pq < K / 2; ++pq) nzr[pq] = nzn[pq] = f2(0.f, 0.f);
+#pragma unroll 4
+      for (int k = 0; k < cnt; ++k) {
+        const double tau = sh.tau[k];
+        const float4 P0 = sh.p0[k], P1 = sh.p1[k], P2 = sh.p2[k], P3 = sh.p3[k];
+        float2 zr[K / 2], zin[K / 2];
+        phasors(tau, P1, P2, P3, zr, zin, true);
+        const float2 Ax = f2(P0.x, P0.x), Ay = f2(P0.y, P0.y), Az = f2(P0.z, P0.z), Bz = f2(P0.w, P0.w);
+        const float2 Axn = f2(P1.x, P1.x), Ayn = f2(P1.y, P1.y), Azn = f2(P1.z, P1.z);
+#pragma unroll
+        for (int pq = 0; pq < K / 2; ++pq) {
+          acc[pq][0] = fma2(Ax, zr[pq], acc[pq][0]);
+          acc[pq][1] = fma2(Axn, zin[pq], acc[pq][1]);
+          acc[pq][2] = fma2(Ay, zr[pq], acc[pq][2]);
+          acc[pq][3] = fma2(Ayn, zin[pq], acc[pq][3]);
+          acc[pq][4] = fma2(Az, zr[pq], acc[pq][4]);
+          acc[pq][5] = fma2(Azn, zin[pq], acc[pq][5]);
+          nzr[pq] = fma2(Bz, zr[pq], nzr[pq]);
+          nzn[pq] = fma2(Bz, zin[pq], nzn[pq]);
+        }
+      }
+      // E_z += i kap sum b_z z: Re += kap sum b_z (-Im z), Im += kap sum b_z Re z
 #pragma unroll
       for (int pq = 0; pq < K / 2; ++pq) {
-        // e += (a + i kap b') z, kap = -c/w per energy
-        const float2 cx = mul2(kap2[pq], Bx), cy = mul2(kap2[pq], By), cz = mul2(kap2[pq], Bz);
-        acc[pq][0] = fma2(Ax, zr[pq], fma2(neg2(cx), zi[pq], acc[pq][0]));
-        acc[pq][1] = fma2(Ax, zi[pq], fma2(cx, zr[pq], acc[pq][1]));
-        acc[pq][2] = fma2(Ay, zr[pq], fma2(neg2(cy), zi[pq], acc[pq][2]));
-        acc[pq][3] = fma2(Ay, zi[pq], fma2(cy, zr[pq], acc[pq][3]));
-        acc[pq][4] = fma2(Az, zr[pq], fma2(neg2(cz), zi[pq], acc[pq][4]));
-        acc[pq][5] = fma2(Az, zi[pq], fma2(cz, zr[pq], acc[pq][5]));
+        acc[pq][4] = fma2(kap2[pq], nzn[pq], acc[pq][4]);
+        acc[pq][5] = fma2(kap2[pq], nzr[pq], acc[pq][5]);
+      }
+    } else {
+      // any energy grid, every component with its near-field term: e += (a + i kap b) z
+#pragma unroll 2
+      for (int k = 0; k < cnt; ++k) {
+        const double tau = sh.tau[k];
+        const float4 P0 = sh.p0[k], P1 = sh.p1[k], P2 = sh.p2[k], P3 = sh.p3[k];
+        float2 zr[K / 2], zin[K / 2];
+        phasors(tau, P1, P2, P3, zr, zin, uniform);
+        const float2 Ax = f2(P0.x, P0.x), Ay = f2(P0.y, P0.y), Az = f2(P0.z, P0.z);
+        const float2 Axn = f2(P1.x, P1.x), Ayn = f2(P1.y, P1.y), Azn = f2(P1.z, P1.z);
+        const float2 Bx = f2(P3.y, P3.y), By = f2(P3.z, P3.z), Bz = f2(P0.w, P0.w);
+#pragma unroll
+        for (int pq = 0; pq < K / 2; ++pq) {
+          const float2 cx = mul2(kap2[pq], Bx), cy = mul2(kap2[pq], By), cz = mul2(kap2[pq], Bz);
+          acc[pq][0] = fma2(Ax, zr[pq], fma2(cx, zin[pq], acc[pq][0]));
+          acc[pq][1] = fma2(Axn, zin[pq], fma2(cx, zr[pq], acc[pq][1]));
+          acc[pq][2] = fma2(Ay, zr[pq], fma2(cy, zin[pq], acc[pq][2]));
+          acc[pq][3] = fma2(Ayn, zin[pq], fma2(cy, zr[pq], acc[pq][3]));
+          acc[pq][4] = fma2(Az, zr[pq], fma2(cz, zin[pq], acc[pq][4]));
+          acc[pq][5] = fma2(Azn, zin[pq], fma2(cz, zr[pq], acc[pq][5]));
+        }
       }
     }
 #pragma unroll

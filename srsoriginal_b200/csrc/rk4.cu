@@ -280,15 +280,19 @@ __global__ void field_eval_kernel(const srs_field *__restrict__ fields, int nfie
 }  // namespace
 
 // Lanes per particle: at least 2 * nfields (two positions per round, one field per lane), rounded
-// up to a power of two; then as many as keep the warps at <= 16 per SM, since wider groups store a
-// point's nine components in parallel and shorten the per-step chain, while narrower groups serve
-// more particles per instruction once there are enough particles to fill the SMs.  G = 32 gives a
-// particle a whole block (four warps sharing the stores), so it is taken only while that fits.
+// up to a power of two; then wider while the particles' groups still fit about one warp per
+// scheduler (148 SMs x 4): wider groups store a point's nine components in parallel and shorten the
+// per-step chain, but once every scheduler has a warp the batch is bound by the instructions issued
+// per particle, which narrower groups save (4096 particles of 20001 points: 16 lanes 35.0 ms, 8
+// lanes 26.3 ms, 4 lanes 25.3 ms, 2 lanes 26.9 ms; 2048: 16 lanes 25.0 ms, 8 lanes 23.1 ms).  G = 32
+// gives a particle a whole block (four warps sharing the stores), taken while blocks of that kind fit
+// 16 warps per SM.
 static int group_size(int nparticles, int nfields) {
-  constexpr int64_t kLanes = (int64_t)148 * 16 * 32;  // 16 warps per SM
+  constexpr int64_t kLanes = (int64_t)148 * 16 * 32;   // 16 warps per SM
+  constexpr int64_t kOneWarpPerScheduler = (int64_t)148 * 4 * 32;
   int G = 2;
   while (G < 2 * nfields) G *= 2;
-  while (G < 16 && (int64_t)nparticles * (2 * G) <= kLanes) G *= 2;
+  while (G < 16 && (int64_t)nparticles * (2 * G) <= kOneWarpPerScheduler) G *= 2;
   if (G == 16 && (int64_t)nparticles * 4 * 32 <= kLanes) G = 32;
   return G;
 }

@@ -475,6 +475,24 @@ def test_spectrum_mixed_within_tolerance():
     assert_mixed(f, f2)
 
 
+@pytest.mark.parametrize("obs, lo, hi, ne", [([0, 0, 30], 100.0, 1000.0, 700),   # x, y near field left out
+                                               ([0.002, -0.001, 3], 10.0, 60.0, 500),  # kept in the drifts
+                                               ([0, 0, 1], 5.0, 20.0, 300)])           # kept nearly everywhere
+def test_spectrum_mixed_near_field_paths(obs, lo, hi, ne):
+    """The mixed spectrum tile leaves out a sub-tile's x, y near-field terms only when they can reach at
+    most 1e-10 of its sum of |a|: observers at 30 m (left out everywhere), 3 m at 10-60 eV (kept in the
+    drifts) and 1 m at 5-20 eV (kept nearly everywhere) all agree with the plain FP64 kernel; so does a
+    non-uniform grid of the same size (one sincos per term, every near-field term kept)."""
+    o = new_sr(20001)
+    _, f = o.spectrum_arrays(obs, ne, [lo, hi], precision="mixed")
+    _, f64 = o.spectrum_arrays(obs, ne, [lo, hi], precision="fp64")
+    assert_mixed(f, f64)
+    pts = np.sort(np.random.default_rng(7).uniform(lo, hi, ne)).tolist()
+    _, f = o.spectrum_arrays(obs, points_eV=pts, precision="mixed")
+    _, f64 = o.spectrum_arrays(obs, points_eV=pts, precision="fp64")
+    assert_mixed(f, f64)
+
+
 def test_beam_spectrum_cfg3a_subsample():
     """Config 3a at its shape (20001-point trajectories, 2000 energies over 100-1000 eV, weight
     1/nparticles) on the reference's own 32-particle subsample from set_seed(0): plain FP64 end to end,
