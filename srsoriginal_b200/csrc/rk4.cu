@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(128) rk4_warp_kernel(const srs_field *__restri
                                                        double *__restrict__ X, double *__restrict__ Bt,
                                                        double *__restrict__ A, const TrajSpec *__restrict__ specs,
                                                        int64_t stage_doubles, const int *__restrict__ skip) {
+  wait_for_previous_grid();  // (launched with launch_after after the parallel-in-time passes)
   if (skip && *skip) return;  // the parallel-in-time integration already wrote this trajectory
   __shared__ srs_field sf[kMaxFieldsShared];
   __shared__ Prepared sp[kMaxFieldsShared];
@@ -323,8 +324,12 @@ static cudaError_t launch_warp_rk4_g(const srs_field *d_fields, int nfields, con
   const size_t smem = sizeof(double) * (size_t)stage_doubles;
   if (cudaError_t e = allow_smem(rk4_warp_kernel<G, kE>, smem)) return e;
   const int warps = 4, per_block = G == 32 ? 1 : warps * (32 / G);
-  rk4_warp_kernel<G, kE><<<(nparticles + per_block - 1) / per_block, 32 * warps, smem, s>>>(
-      d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x, d_b, d_a, d_specs, stage_doubles, d_skip);
+  const dim3 grid((nparticles + per_block - 1) / per_block), block(32 * warps);
+  if (d_skip)  // the fallback after the parallel-in-time passes: set up while they finish
+    return launch_after(rk4_warp_kernel<G, kE>, grid, block, smem, s, d_fields, nfields, d_particles, nparticles, dt,
+                        nfwd, nbwd, d_x, d_b, d_a, d_specs, stage_doubles, d_skip);
+  rk4_warp_kernel<G, kE><<<grid, block, smem, s>>>(d_fields, nfields, d_particles, nparticles, dt, nfwd, nbwd, d_x,
+                                                   d_b, d_a, d_specs, stage_doubles, d_skip);
   return cudaGetLastError();
 }
 

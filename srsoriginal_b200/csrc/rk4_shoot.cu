@@ -96,6 +96,7 @@ struct Scratch {
 
 __global__ void shoot_init_kernel(Plan P, const srs_particle *__restrict__ part, Scratch W,
                                   const srs_field *__restrict__ fields, int nfields) {
+  allow_next_grid();  // the first pass may be set up meanwhile (it waits for this grid's writes)
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < nfields) prepare(fields[g], W.prep[g]);  // once per integration, not once per pass and block
   if (g == 0) {
@@ -460,6 +461,10 @@ __global__ void __launch_bounds__(kShootThreads) shoot_pass_kernel(const srs_fie
                                                                    double *__restrict__ Bt, double *__restrict__ A,
                                                                    int64_t stage_doubles, int final_pass) {
   __shared__ PassShared<kShootThreads / G> sh;
+  // launched as a programmatic dependent of the previous kernel (launch_after): wait until that grid
+  // has completed and its writes are visible, then let the next launch begin while this one runs
+  wait_for_previous_grid();
+  allow_next_grid();
   const int conv = W.flags[0], near = W.flags[2], stored = W.flags[3];
   if (final_pass) {
     if (conv && !stored) shoot_pass<G, false>(sh, gfields, nfields, part, P, W, X, Bt, A, stage_doubles, true);
@@ -541,9 +546,8 @@ cudaError_t launch_pass(int blocks, size_t smem, cudaStream_t s, const srs_field
     if (cudaError_t e = cudaFuncSetAttribute(shoot_pass_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem))
       return e;
-  shoot_pass_kernel<G><<<blocks, kShootThreads, smem, s>>>(d_fields, nfields, d_particle, P, W, d_x, d_b, d_a,
-                                                           stage_doubles, final_pass);
-  return cudaGetLastError();
+  return launch_after(shoot_pass_kernel<G>, dim3((unsigned)blocks), dim3(kShootThreads), smem, s, d_fields, nfields,
+                      d_particle, P, W, d_x, d_b, d_a, stage_doubles, final_pass);
 }
 
 cudaError_t launch_pass_g(int G, int blocks, size_t smem, cudaStream_t s, const srs_field *d_fields, int nfields,

@@ -24,6 +24,32 @@ srs_status cuda_fail(cudaError_t e, const char *what);
     if (srs_e_ != cudaSuccess) return ::srs::cuda_fail(srs_e_, #call); \
   } while (0)
 
+// ---- programmatic dependent launch ----
+// A kernel launched by launch_after may be set up on the GPU while the stream's previous kernel is
+// still running; it must call wait_for_previous_grid() before it reads or writes any memory that
+// kernel touches (the wait ends when that grid has completed and its writes are visible; in a kernel
+// launched the ordinary way it returns at once).  allow_next_grid() lets the stream's next such launch
+// begin early.  Used on chains of short dependent kernels (the parallel-in-time passes, then the sums),
+// where the launch latency between kernels is a visible part of the time.
+__device__ __forceinline__ void wait_for_previous_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_after(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // The library's stream-ordered memory pool of the current device (created on first use, kept for the
 // process).  Freed blocks stay in it for the next call instead of going back to the driver at every
 // synchronisation (a pool's default release threshold is 0, which makes a call that needs the 5.9 GB

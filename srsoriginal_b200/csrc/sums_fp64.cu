@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(6 * kRedPoints) flux_fp64_reduce(const double 
                                                                    double dt, double C0, double C2,
                                                                    double *__restrict__ out, double *__restrict__ e6) {
   __shared__ double se[kRedPoints][7];
+  wait_for_previous_grid();  // (launched with launch_after by finish_flux_partials)
   const int k = threadIdx.x % kRedPoints, c = threadIdx.x / kRedPoints;
   const int64_t idx = (int64_t)blockIdx.x * kRedPoints + k;
   const bool valid = idx < np * nparticles;
@@ -432,9 +433,9 @@ cudaError_t total_power(const srs_traj_view &t, const srs_beam_consts &b, const 
 cudaError_t finish_flux_partials(const double *partial, int S, int64_t nout, int nparticles, const double *omegas,
                                  double omega0, double dt, double C0, double C2, double *out, cudaStream_t s,
                                  double *e6) {
-  flux_fp64_reduce<<<blocks_for(nout * nparticles, kRedPoints), 6 * kRedPoints, 0, s>>>(partial, S, nout, nparticles, omegas, omega0, dt,
-                                                                     C0, C2, out, e6);
-  return cudaGetLastError();
+  // set up while the sums that wrote the partials finish (the kernel waits for their writes)
+  return launch_after(flux_fp64_reduce, dim3((unsigned)blocks_for(nout * nparticles, kRedPoints)),
+                      dim3(6 * kRedPoints), 0, s, partial, S, nout, nparticles, omegas, omega0, dt, C0, C2, out, e6);
 }
 
 cudaError_t finish_pd_partials(const double *partial, int S, int64_t np, int nparticles, double cdt, int directional,

@@ -50,6 +50,8 @@ __global__ void __launch_bounds__(kThreads, 6) flux_mixed_kernel(const double *_
                                                               double omega, int64_t chunk,
                                                               double *__restrict__ partial) {
   __shared__ tiles::FluxShared sh;
+  wait_for_previous_grid();  // (launched with launch_after by the one-shot launcher)
+  allow_next_grid();
   const int s = blockIdx.y, S = gridDim.y, p = blockIdx.z;
   const int64_t np = (int64_t)g.n1 * g.n2;
   const int64_t i0 = (int64_t)s * chunk;
@@ -382,8 +384,9 @@ static cudaError_t mixed_flux_splits(const srs_traj_view &t, const srs_beam_cons
   const double omega = ev_to_omega(energy_ev);
   double *partial = static_cast<double *>(scratch);
   dim3 grid((unsigned)m.tiles, S, t.nparticles);
-  flux_mixed_kernel<<<grid, kThreads, 0, s>>>(t.x, t.beta, t.n, t.dt, g, m, omega, chunk, partial);
-  cudaError_t e = cudaGetLastError();
+  // set up while the trajectory's last kernel finishes (the kernel waits for its writes)
+  cudaError_t e = launch_after(flux_mixed_kernel, grid, dim3(kThreads), 0, s, t.x, t.beta, t.n, t.dt, g, m, omega,
+                               chunk, partial);
   if (e != cudaSuccess) return e;
   return finish_flux_partials(partial, S, (int64_t)g.n1 * g.n2, t.nparticles, nullptr, omega, t.dt, flux_c0(b.charge),
                               flux_c2(b.charge, b.current), d_out, s);
