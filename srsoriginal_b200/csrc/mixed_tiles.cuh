@@ -20,28 +20,6 @@ constexpr int kThreads = 128;
 constexpr int kSub = 128;               // trajectory points per shared-memory tile
 constexpr int kEnergiesPerThread = 4;
 
-// Trajectory chunks S per tile for ctas tiles on a GPU with `slots` resident CTAs per wave: the S
-// minimising the modelled time waves(S) * (n/S + overhead), waves = ceil(ctas * S / slots), with
-// chunks of at least min_chunk points.  A grid that overshoots a whole wave by a few CTAs leaves them
-// to run alone at the end, so the model picks S that fills the last wave instead.
-inline int splits_for(int64_t ctas, int64_t n, int64_t min_chunk, int64_t slots) {
-  ctas = std::max<int64_t>(1, ctas);
-  slots = std::max<int64_t>(1, slots);
-  const int64_t max_s = std::min<int64_t>(std::max<int64_t>(1, n / min_chunk), 4096);
-  constexpr double kOverhead = 64.0;  // per-CTA set-up and output, in trajectory points
-  int best_s = 1;
-  double best = 1e300;
-  for (int64_t s = 1; s <= max_s; ++s) {
-    const int64_t waves = (ctas * s + slots - 1) / slots;
-    const double cost = (double)waves * ((double)((n + s - 1) / s) + kOverhead);
-    if (cost < best * (1.0 - 1e-9)) {
-      best = cost;
-      best_s = (int)s;
-    }
-  }
-  return best_s;
-}
-
 // Trajectory points per chunk for S chunks, rounded up to whole shared-memory sub-tiles: the FP32
 // accumulators restart at every sub-tile, so with sub-tile-aligned chunks the result depends on S
 // only through the FP64 order of the per-chunk sums.  The chunks actually used are ceil(n / chunk).
@@ -50,6 +28,51 @@ inline int64_t aligned_chunk(int64_t n, int S) {
   return (c + kSub - 1) / kSub * kSub;
 }
 inline int used_chunks(int64_t n, int64_t chunk) { return (int)((n + chunk - 1) / chunk); }
+
+// Trajectory chunks S per tile for ctas tiles on a GPU with `slots` resident CTAs per wave, with chunks
+// of at least min_chunk points.  Modelled time of a split: waves * (chunk + overhead) for the chunks
+// the launch will actually use (aligned_chunk), waves = ceil(ctas * used / slots): a grid that
+// overshoots a whole wave by a few CTAs leaves them to run alone at the end, so the model favours
+// splits that fill the last wave.  The model does not see how a partly filled last wave drains, nor
+// the per-chunk partial sums, so among splits within 2 % of the best: the finest when the best takes
+// few waves (< 8: a long last CTA then decides the end), the coarsest otherwise (fewer partials).
+// Measured on the config-1 map (81 tiles x 20001 points, 888 slots): 10 chunks 0.308 ms, 16 0.283,
+// 20 0.276, 27 0.281, 32 0.269 (picked), 40 0.275; config 2 (318 tiles x 40001 points, 740 slots):
+// 16 chunks 3.04 ms (picked), 9 chunks 3.11 ms.
+inline int splits_for(int64_t ctas, int64_t n, int64_t min_chunk, int64_t slots) {
+  ctas = std::max<int64_t>(1, ctas);
+  slots = std::max<int64_t>(1, slots);
+  const int64_t max_s = std::min<int64_t>(std::max<int64_t>(1, n / min_chunk), 4096);
+  constexpr double kOverhead = 64.0;  // per-CTA set-up and output, in trajectory points
+  constexpr double kTol = 0.02;
+  auto model = [&](int64_t s, int64_t &used, int64_t &waves) {
+    const int64_t chunk = aligned_chunk(n, (int)s);
+    used = used_chunks(n, chunk);
+    waves = (ctas * used + slots - 1) / slots;
+    return (double)waves * ((double)chunk + kOverhead);
+  };
+  double best = 1e300;
+  int64_t best_waves = 1, used = 0, waves = 0;
+  for (int64_t s = 1; s <= max_s; ++s) {
+    const double c = model(s, used, waves);
+    if (c < best) {
+      best = c;
+      best_waves = waves;
+    }
+  }
+  const bool finest = best_waves < 8;
+  int best_s = 1;
+  int64_t pick_used = finest ? 0 : INT64_MAX;
+  for (int64_t s = 1; s <= max_s; ++s) {
+    const double c = model(s, used, waves);
+    if (c > best * (1.0 + kTol)) continue;
+    if (finest ? used > pick_used : used < pick_used) {
+      pick_used = used;
+      best_s = (int)s;
+    }
+  }
+  return best_s;
+}
 
 // Resident CTAs of `kernel` (kThreads threads, no dynamic shared memory) on the current device,
 // queried once per (kernel, device): the launchers ask on every call.
