@@ -107,6 +107,20 @@ static int check_chunks() {
       if (s < 1 || s > std::max<int64_t>(1, n / 256)) ++bad;
     }
   }
+  // the splits measured fastest on a B200: the config-1 map (81 strip tiles, 20001 points, 6 CTAs per
+  // SM) in 32 chunks of 640 points, config 2's power density (318 tiles, 40001 points, 5 CTAs per SM)
+  // in 16 chunks of 2560
+  auto used_for = [](int64_t ctas, int64_t n, int64_t slots) {
+    return used_chunks(n, aligned_chunk(n, splits_for(ctas, n, 256, slots)));
+  };
+  if (used_for(81, 20001, 148 * 6) != 32) {
+    std::printf("config-1 split: %d chunks\n", used_for(81, 20001, 148 * 6));
+    ++bad;
+  }
+  if (used_for(318, 40001, 148 * 5) != 16) {
+    std::printf("config-2 split: %d chunks\n", used_for(318, 40001, 148 * 5));
+    ++bad;
+  }
   return bad;
 }
 
