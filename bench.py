@@ -331,6 +331,38 @@ def _events_ms(fn, reps, warmup=1):
     return statistics.median(times)
 
 
+def _graph_ms(fn, reps=20):
+    """Device time [ms] of one fn() without the host's launch overhead: fn captured once into a CUDA
+    graph, the graph replayed reps times back to back, CUDA events around the replays.  None if the
+    calls cannot be captured."""
+    import torch
+    try:
+        fn()
+        torch.cuda.synchronize()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            fn()
+        torch.cuda.current_stream().wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            fn()
+        g.replay()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            g.replay()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / reps
+        del g
+        return ms
+    except Exception as ex:  # capture of a library call that allocates or synchronises
+        log(f"graph timing unavailable: {ex}")
+        return None
+
+
 def measure_configs(dev, peaks=None):
     """The other configurations' throughput, for the record (not the headline): each device-timed
     with CUDA events (median of a few runs) unless marked wall-clock."""
@@ -356,8 +388,14 @@ def measure_configs(dev, peaks=None):
     spm = torch.empty_like(sp)
     D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, spm, precision=_lib.MIXED)
     D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sp, precision=_lib.FP64)
+    # the same calls replayed from a CUDA graph: the device time without the per-call host overhead,
+    # which is a large part of a 1000-energy spectrum's time
+    gms = _graph_ms(lambda: D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sp, precision=_lib.FP64))
+    gmsm = _graph_ms(lambda: D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sp, precision=_lib.MIXED))
     out["cfg0_spectrum"] = {"evals": ev, "fp64_ms": ms, "fp64_evals_per_s": ev / (ms * 1e-3), "mixed_ms": msm,
-                            "mixed_evals_per_s": ev / (msm * 1e-3),
+                            "mixed_evals_per_s": ev / (msm * 1e-3), "fp64_graph_ms": gms, "mixed_graph_ms": gmsm,
+                            "graph_note": "one call captured in a CUDA graph and replayed back to back: device time "
+                                          "without the per-call launch overhead",
                             "mixed_error_vs_fp64": error_floors(spm.cpu().numpy(), sp.cpu().numpy())}
 
     # the trajectory: serial RK4 chain against the parallel-in-time integration (configs 0/1 and 2)
