@@ -390,8 +390,9 @@ def measure_configs(dev, peaks=None):
     D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sp, precision=_lib.FP64)
     # the same calls replayed from a CUDA graph: the device time without the per-call host overhead,
     # which is a large part of a 1000-energy spectrum's time
-    gms = _graph_ms(lambda: D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sp, precision=_lib.FP64))
-    gmsm = _graph_ms(lambda: D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sp, precision=_lib.MIXED))
+    sg = torch.empty_like(sp)  # (sp and spm hold the results compared below)
+    gms = _graph_ms(lambda: D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sg, precision=_lib.FP64))
+    gmsm = _graph_ms(lambda: D.spectrum(traj, charge, current, [0, 0, W.SCREEN_Z], e0, sg, precision=_lib.MIXED))
     out["cfg0_spectrum"] = {"evals": ev, "fp64_ms": ms, "fp64_evals_per_s": ev / (ms * 1e-3), "mixed_ms": msm,
                             "mixed_evals_per_s": ev / (msm * 1e-3), "fp64_graph_ms": gms, "mixed_graph_ms": gmsm,
                             "graph_note": "one call captured in a CUDA graph and replayed back to back: device time "
