@@ -736,7 +736,8 @@ def run_ours(args, world, rank, local):
     return 0
 
 
-PROFILE_CASES = ("flux_mixed_cfg1", "flux_fp64_cfg1", "pd_fp64_51x51", "spectrum_mixed_3a256", "shoot_cfg1")
+PROFILE_CASES = ("flux_mixed_cfg1", "flux_fp64_cfg1", "pd_fp64_51x51", "spectrum_mixed_3a256", "shoot_cfg1",
+                 "spectrum_cfg0")
 
 
 def run_case(name):
@@ -744,7 +745,8 @@ def run_case(name):
     flux_mixed_cfg1 / flux_fp64_cfg1: the config-1 map at 3*E1 (mixed / plain FP64); pd_fp64_51x51:
     config 2's power density on 51 x 51 points (40001-point trajectory, plain FP64);
     spectrum_mixed_3a256: 256 electrons of config 3a's shape (20001 points, 2000 energies, mixed);
-    shoot_cfg1: the config-1 trajectory integrated parallel in time."""
+    shoot_cfg1: the config-1 trajectory integrated parallel in time; spectrum_cfg0: config 0's
+    1000-energy spectrum, mixed then plain FP64."""
     import numpy as np
     import torch
 
@@ -778,6 +780,12 @@ def run_case(name):
             D.spectrum(tb, charge, current, [0, 0, W.SCREEN_Z], e, out, precision=_lib.MIXED)
         elif name == "shoot_cfg1":
             D.trajectory_shoot(und, part, 0.0, 2.0, 0.0, NT)
+        elif name == "spectrum_cfg0":
+            t1 = D.trajectory(und, [part], 0.0, 2.0, 0.0, NT)
+            e = torch.tensor(energy_grid(1000, 100.0, 1000.0), dtype=torch.float64, device="cuda")
+            out = torch.empty(1000, dtype=torch.float64, device="cuda")
+            D.spectrum(t1, charge, current, [0, 0, W.SCREEN_Z], e, out, precision=_lib.MIXED)
+            D.spectrum(t1, charge, current, [0, 0, W.SCREEN_Z], e, out, precision=_lib.FP64)
         torch.cuda.synchronize()
     log(f"case {name} ok")
     return 0
