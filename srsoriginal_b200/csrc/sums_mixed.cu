@@ -532,8 +532,9 @@ cudaError_t mixed_power_density_points(const srs_traj_view &t, const srs_beam_co
 // Energies per thread and trajectory chunks of a spectrum launch: kEnergiesPerThread with chunks of at
 // least two sub-tiles when those CTAs fill one wave; otherwise (one observer's spectrum of a few
 // thousand energies) two energies per thread and chunks down to one sub-tile, so that more CTAs share
-// the work, but at most 64 chunks (measured: one-sub-tile chunks took a 1000-energy spectrum from
-// 0.095 to 0.088 ms but a 2000-energy one from 0.079 to 0.083 ms).
+// the work (a 1000-energy spectrum: 0.095 -> 0.083 ms per call against chunks of three sub-tiles; the
+// partials, a few MB, stay in L2, and the reduction loads 24 chunks at a time).
+
 struct SpecPlan {
   int K;
   int64_t etiles;
@@ -551,8 +552,7 @@ static SpecPlan spectrum_plan(int64_t n, int64_t ne, int nparticles) {
   } else {
     P.K = 2;
     P.etiles = (ne + kThreads * 2 - 1) / (kThreads * 2);
-    P.S_max = splits_for(P.etiles * nparticles, n, std::max<int64_t>(kSub, (n + 63) / 64),
-                         wave_slots(spectrum_mixed_kernel<2>));
+    P.S_max = splits_for(P.etiles * nparticles, n, (int64_t)kSub, wave_slots(spectrum_mixed_kernel<2>));
   }
   return P;
 }
