@@ -478,11 +478,21 @@ def measure_configs(dev, peaks=None):
     e3a = torch.tensor(energy_grid(2000, 100.0, 1000.0), dtype=torch.float64, device=dev)
     s3a = torch.empty(4096 * 2000, dtype=torch.float64, device=dev)
     sum_ms = _events_ms(lambda: D.spectrum(tb, charge, current, [0, 0, W.SCREEN_Z], e3a, s3a, precision=_lib.MIXED), 3)
-    del tb, s3a
+    # the same 4096 spectra as 4096 jobs of the persistent work queue (one graph launch over (job,
+    # energy tile, trajectory chunk) items), on the same trajectories
+    qjobs = [Q.spectrum_job(D.Trajectory(tb.x[p:p + 1], tb.beta[p:p + 1], tb.aoc[p:p + 1], tb.dt), charge, current,
+                            [0, 0, W.SCREEN_Z], e3a, s3a[p * 2000:(p + 1) * 2000]) for p in range(4096)]
+    q3a = Q.JobQueue(qjobs, chunk=8192, energies_per_thread=4)
+    q3a_ms = _events_ms(q3a.run, 3)
+    q3a.close()
+    del qjobs, q3a, tb, s3a
     out["cfg3a_beam_spectrum"] = {"evals": ev, "wall_s": wall, "wall_s_all": walls, "evals_per_s": ev / wall,
                                   "includes": "public API call: sampling, 4096 RK4, mixed sums, accumulation",
                                   "rk4_batch_ms": rk_ms, "spectrum_sums_ms": sum_ms,
                                   "spectrum_sums_evals_per_s": ev / (sum_ms * 1e-3),
+                                  "queue_sums_ms": q3a_ms,
+                                  "queue_note": "the 4096 spectra as 4096 jobs of the persistent work queue (chunk "
+                                                "8192, four energies per thread), one CUDA-graph launch",
                                   "spectrum_sums_fp32_frac_of_measured_peak": (
                                       _COUNTS["spectrum_uniform_mixed"]["fp32"] * ev / (sum_ms * 1e-3)
                                       / peaks["fp32"] if peaks else None),
