@@ -534,8 +534,9 @@ def measure_configs(dev, peaks=None):
     qs.close()
     del jobs, trajs, jobs_s, trajs_s
 
-    # config 4: adjoint / forward time (forward = RK4 through the 2001-sample grid + mixed spectrum of
-    # 200 energies; adjoint = sum adjoint + trajectory adjoint scan, FP64)
+    # config 4: adjoint / forward time (forward = the trajectory through the 2001-sample grid, parallel in
+    # time, + mixed spectrum of 200 energies; adjoint = the E_k re-formed in FP64, sum adjoint +
+    # trajectory adjoint scan, FP64)
     problem, grid, ic, de = W.config4_problem(precision=_lib.MIXED)
     fw, bw = [], []
     gfl = None
@@ -747,7 +748,7 @@ def run_ours(args, world, rank, local):
 
 
 PROFILE_CASES = ("flux_mixed_cfg1", "flux_fp64_cfg1", "pd_fp64_51x51", "spectrum_mixed_3a256", "shoot_cfg1",
-                 "spectrum_cfg0")
+                 "spectrum_cfg0", "adjoint_cfg4")
 
 
 def run_case(name):
@@ -756,7 +757,7 @@ def run_case(name):
     config 2's power density on 51 x 51 points (40001-point trajectory, plain FP64);
     spectrum_mixed_3a256: 256 electrons of config 3a's shape (20001 points, 2000 energies, mixed);
     shoot_cfg1: the config-1 trajectory integrated parallel in time; spectrum_cfg0: config 0's
-    1000-energy spectrum, mixed then plain FP64."""
+    1000-energy spectrum, mixed then plain FP64; adjoint_cfg4: config 4's forward and adjoint."""
     import numpy as np
     import torch
 
@@ -790,6 +791,11 @@ def run_case(name):
             D.spectrum(tb, charge, current, [0, 0, W.SCREEN_Z], e, out, precision=_lib.MIXED)
         elif name == "shoot_cfg1":
             D.trajectory_shoot(und, part, 0.0, 2.0, 0.0, NT)
+        elif name == "adjoint_cfg4":
+            from srsoriginal_b200.adjoint import backward_flux, forward_flux
+            problem, grid4, ic4, de4 = W.config4_problem()
+            f4, saved4 = forward_flux(problem, grid4, None, ic4, keep_efield=True)
+            backward_flux(problem, saved4, torch.full_like(f4, -de4))
         elif name == "spectrum_cfg0":
             t1 = D.trajectory(und, [part], 0.0, 2.0, 0.0, NT)
             e = torch.tensor(energy_grid(1000, 100.0, 1000.0), dtype=torch.float64, device="cuda")

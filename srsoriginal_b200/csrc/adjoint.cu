@@ -32,6 +32,8 @@
 // run-to-run differences); everything else is reduced in a fixed order.
 #include <cuda_runtime.h>
 
+#include <cuda_pipeline.h>
+
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -423,8 +425,15 @@ __global__ void chunk_compose_kernel(Traj T, Chains C, const double *__restrict_
   }
 }
 
-// (c) one warp per chain, lanes 0..5 own one component: lambda at every chunk start.
-__global__ void carry_kernel(Traj T, Chains C, const double *__restrict__ Mb, double *__restrict__ lam0) {
+// (c) one warp per chain, lanes 0..5 own one component: lambda at every chunk start.  The sweep is
+// sequential over the chunks, so the chunk maps come through shared memory in tiles of kCarryTile,
+// the next tile's asynchronous copies in flight while the current one is swept (a step then waits on
+// shared memory, not on a global load: 1250 chunks of config 4 took 0.63 ms with the maps read from
+// global memory step by step).
+constexpr int kCarryTile = 64;  // chunk maps per tile: 64 x 42 doubles = 21.5 KB, two buffers
+__global__ void __launch_bounds__(32) carry_kernel(Traj T, Chains C, const double *__restrict__ Mb,
+                                                   double *__restrict__ lam0) {
+  __shared__ __align__(16) double tile[2][kCarryTile * 42];
   const int chain = blockIdx.x;
   if (chain >= C.n) return;
   const Chain &ch = C.c[chain];
@@ -432,15 +441,42 @@ __global__ void carry_kernel(Traj T, Chains C, const double *__restrict__ Mb, do
   double g[6];
   load_g(T, ch, ch.L - 1, g);
   double lam = r < 6 ? g[r] : 0.0;  // lambda_{L-1} = g_{L-1}
-  for (int64_t c = ch.nch - 1; c >= 0; --c) {
-    const double *o = Mb + 42 * (ch.chunk_off + c);
-    double s = r < 6 ? o[36 + r] : 0.0;
-    for (int k = 0; k < 6; ++k) {
-      const double lk = __shfl_sync(0xffffffffu, lam, k);
-      if (r < 6) s += o[6 * r + k] * lk;
+  const int64_t nch = ch.nch, ntiles = (nch + kCarryTile - 1) / kCarryTile;
+  // tile t: chunks [lo(t), hi(t)], hi(t) = nch - 1 - t * kCarryTile, swept from hi down to lo
+  auto lo_of = [&](int64_t t) {
+    const int64_t hi = nch - 1 - t * kCarryTile;
+    return hi - kCarryTile + 1 > 0 ? hi - kCarryTile + 1 : (int64_t)0;
+  };
+  auto fetch = [&](int64_t t, int buf) {  // 16-byte copies: a chunk map is 21 of them, 16-byte aligned
+    const int64_t hi = nch - 1 - t * kCarryTile, lo = lo_of(t);
+    const double *src = Mb + 42 * (ch.chunk_off + lo);
+    const int n16 = (int)(hi - lo + 1) * 21;
+    for (int k = r; k < n16; k += 32) __pipeline_memcpy_async(&tile[buf][2 * k], src + 2 * k, 16);
+    __pipeline_commit();
+  };
+  if (ntiles > 0) fetch(0, 0);
+  for (int64_t t = 0; t < ntiles; ++t) {
+    const int buf = (int)(t & 1);
+    if (t + 1 < ntiles) fetch(t + 1, buf ^ 1);
+    else __pipeline_commit();  // an empty group, so that "all but the newest" is always tile t
+    __pipeline_wait_prior(1);
+    __syncwarp();
+    const int64_t hi = nch - 1 - t * kCarryTile, lo = lo_of(t);
+    const int rr = r < 6 ? r : 0;
+    for (int64_t c = hi; c >= lo; --c) {
+      const double *o = &tile[buf][42 * (c - lo)];
+      double l[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) l[k] = __shfl_sync(0xffffffffu, lam, k);
+      // b + M lambda as a tree (depth 4 instead of a chain of six multiply-adds: the sweep is a chain
+      // of these, one per chunk)
+      const double *m = o + 6 * rr;
+      const double p0 = m[0] * l[0], p1 = m[1] * l[1], p2 = m[2] * l[2], p3 = m[3] * l[3], p4 = m[4] * l[4],
+                   p5 = m[5] * l[5];
+      lam = o[36 + rr] + (((p0 + p1) + (p2 + p3)) + (p4 + p5));
+      if (r < 6) lam0[6 * (ch.chunk_off + c) + r] = lam;
     }
-    lam = s;
-    if (r < 6) lam0[6 * (ch.chunk_off + c) + r] = lam;
+    __syncwarp();  // every lane is done with this buffer before the next iteration refills it
   }
 }
 
@@ -491,24 +527,34 @@ __global__ void __launch_bounds__(64) chunk_finish_kernel(const srs_field *__res
     for (int r = 0; r < 6; ++r) lam_init[6 * chain + r] = lam[r];
 }
 
-// Fixed-order totals: out[0..2] dL/dx0, out[3..5] dL/dbeta0, out[6] dL/dq, out[7..] amplitudes.
-__global__ void adjoint_total_kernel(Chains C, int nf, const double *__restrict__ lam_init,
-                                     const double *__restrict__ amp_part, const double *__restrict__ q_part,
-                                     double *__restrict__ out) {
+// Fixed-order totals: out[0..2] dL/dx0, out[3..5] dL/dbeta0, out[6] dL/dq, out[7..] amplitudes.  The
+// per-chunk partials of q and of each amplitude are added by the block: thread t adds a contiguous
+// run of chunks in order, then a fixed tree over the 128 runs (a deterministic order; one thread
+// adding all 1250 partials of config 4 one load after another took 0.12 ms).
+__global__ void __launch_bounds__(128) adjoint_total_kernel(Chains C, int nf, const double *__restrict__ lam_init,
+                                                            const double *__restrict__ amp_part,
+                                                            const double *__restrict__ q_part,
+                                                            double *__restrict__ out) {
+  __shared__ double red[128];
   const int t = threadIdx.x;
   if (t < 6) {
     double s = 0.0;
     for (int k = 0; k < C.n; ++k) s += lam_init[6 * k + t];
     out[t] = s;
-  } else if (t == 6) {
+  }
+  const int64_t total = C.total_chunks, per = (total + 127) / 128;
+  const int64_t g0 = t * per, g1 = g0 + per < total ? g0 + per : total;
+  for (int o = 0; o < 1 + 3 * nf; ++o) {  // o = 0: q; o = 1 + i: amplitude i
     double s = 0.0;
-    for (int64_t g = 0; g < C.total_chunks; ++g) s += q_part[g];
-    out[6] = s;
-  } else if (t < 7 + 3 * nf) {
-    const int i = t - 7;
-    double s = 0.0;
-    for (int64_t g = 0; g < C.total_chunks; ++g) s += amp_part[(int64_t)3 * nf * g + i];
-    out[t] = s;
+    for (int64_t g = g0; g < g1; ++g) s += o == 0 ? q_part[g] : amp_part[(int64_t)3 * nf * g + (o - 1)];
+    red[t] = s;
+    __syncthreads();
+    for (int w = 64; w > 0; w >>= 1) {
+      if (t < w) red[t] += red[t + w];
+      __syncthreads();
+    }
+    if (t == 0) out[6 + o] = red[0];
+    __syncthreads();
   }
 }
 
