@@ -523,8 +523,9 @@ struct SpecShared {
 constexpr float kNearPerp = 1e-10f;
 
 // x modulo 2 pi for the spectrum's per-(point, thread) phase: the Cody-Waite steps of reduce_2pi
-// without its third part, whose product k * P3 is below 1e-20 rad for |x| < 1e13 rad (phases here are
-// at most ~1e12 rad), so the result equals reduce_2pi's to within an ulp of pi.
+// without its third part, whose product k * P3 is below |x| * 1e-33 rad (1e-18 rad for |x| < 1e15
+// rad, while the FP64 phase w tau itself carries |x| * 1.1e-16), so the result equals reduce_2pi's to
+// within an ulp of pi.
 __device__ __forceinline__ double reduce_2pi_short(double x) {
   const double kInv2Pi = 0.15915494309189535;
   const double P1 = 6.283185307179586, P2 = 2.4492935982947064e-16;
