@@ -493,6 +493,29 @@ def test_spectrum_mixed_near_field_paths(obs, lo, hi, ne):
     assert_mixed(f, f64)
 
 
+def test_spectrum_mixed_batched_near_observer_and_nonuniform():
+    """Four energies per thread (the batched launch: 8 particles, 4096 energies) on the paths the
+    30-m tests do not take: an observer 3 m away at 10-60 eV (sub-tiles that keep the x, y near-field
+    terms) and a non-uniform grid (one sincos per term); against the plain FP64 kernel, per particle."""
+    import torch
+    from srsoriginal_b200 import _lib, device as D
+    from srsoriginal_b200.sr import energy_grid
+    part, _ = D.ideal_particle(W.ENERGY_GEV, [0, 0, -1], [0, 0, 1])
+    und = [D.undulator([0, W.BPEAK, 0], [0, 0, W.PERIOD], W.NPERIODS)]
+    tb = D.trajectory(und, [part] * 8, 0.0, 2.0, 0.0, 20001)
+    uniform = energy_grid(4096, 10.0, 60.0)
+    ragged = np.sort(np.random.default_rng(11).uniform(10.0, 60.0, 4096))
+    for ev in (uniform, ragged):
+        e = torch.tensor(ev, dtype=torch.float64, device="cuda")
+        fm = torch.empty(8 * 4096, dtype=torch.float64, device="cuda")
+        f64 = torch.empty_like(fm)
+        D.spectrum(tb, -D.QE, W.CURRENT, [0.002, -0.001, 3.0], e, fm, precision=_lib.MIXED)
+        D.spectrum(tb, -D.QE, W.CURRENT, [0.002, -0.001, 3.0], e, f64, precision=_lib.FP64)
+        a, b = fm.cpu().numpy().reshape(8, -1), f64.cpu().numpy().reshape(8, -1)
+        for p in range(8):
+            assert_mixed(a[p], b[p])
+
+
 def test_beam_spectrum_cfg3a_subsample():
     """Config 3a at its shape (20001-point trajectories, 2000 energies over 100-1000 eV, weight
     1/nparticles) on the reference's own 32-particle subsample from set_seed(0): plain FP64 end to end,
